@@ -1,0 +1,170 @@
+"""B200-native tripartite neuron-astrocyte network simulator.
+
+Python host side of the C ABI in include/astrosim.h (library
+``lib/libastrosim_b200.so``, built by ``make -C astrosimgpu_cuda_b200`` or
+``__graft_entry__.build()``).  The reference program (src/astrosim_fused.cu)
+exposes only a CLI; :class:`Simulation` mirrors its run structure
+(create -> step -> summary) on top of the library, and every computation runs in
+the library's CUDA kernels.  There is no CPU path: importing works without a
+GPU, but creating a simulation needs the built library and a CUDA device.
+"""
+import ctypes as C
+import math
+import os
+import subprocess
+
+import numpy as np
+
+from . import abi
+from .abi import default_config, scaling  # noqa: F401
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_DIR = os.path.join(HERE, "lib")
+LIB_PATH = os.path.join(LIB_DIR, "libastrosim_b200.so")
+CLI_PATH = os.path.join(LIB_DIR, "astrosim")
+
+_lib = None
+
+
+class AstrosimError(RuntimeError):
+    """A library call returned a non-zero status."""
+
+    def __init__(self, code, msg):
+        super().__init__(f"astrosim error {code}: {msg}")
+        self.code = code
+
+
+def build(jobs=8):
+    """Compiles the CUDA library and the CLI for sm_100a (nvcc; no GPU needed)."""
+    subprocess.run(["make", "-s", "-C", HERE, f"-j{jobs}"], check=True)
+
+
+def lib():
+    """Loads the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `make -C {HERE}` "
+                          "(the simulator has no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    P = C.c_void_p
+    u32p = C.POINTER(C.c_uint32)
+    L.astrosim_config_default.argtypes = [C.POINTER(abi.Config)]
+    L.astrosim_config_default.restype = None
+    L.astrosim_last_error.restype = C.c_char_p
+    L.astrosim_abi_version.restype = C.c_int
+    L.astrosim_create.argtypes = [C.POINTER(abi.Config), C.POINTER(P)]
+    L.astrosim_step.argtypes = [P, C.c_int64]
+    L.astrosim_summary.argtypes = [P, C.POINTER(abi.Summary)]
+    L.astrosim_destroy.argtypes = [P]
+    L.astrosim_spike_counts.argtypes = [P, C.c_int64, C.c_int64, u32p]
+    L.astrosim_raster.argtypes = [P, u32p, C.c_size_t]
+    L.astrosim_get_state.argtypes = [P, C.c_int, C.POINTER(C.c_double), C.c_size_t]
+    L.astrosim_get_csr.argtypes = [P, C.c_int, u32p, C.c_size_t, u32p, C.c_size_t,
+                                   C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]
+    L.astrosim_dump_edges.argtypes = [P, C.c_char_p]
+    L.astrosim_last_step_ms.argtypes = [P, C.POINTER(C.c_double)]
+    L.astrosim_device_info.argtypes = [C.c_int, C.c_char_p, C.c_size_t, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    for name in ("astrosim_create", "astrosim_step", "astrosim_summary", "astrosim_destroy",
+                 "astrosim_spike_counts", "astrosim_raster", "astrosim_get_state", "astrosim_get_csr",
+                 "astrosim_dump_edges", "astrosim_last_step_ms", "astrosim_device_info"):
+        getattr(L, name).restype = C.c_int
+    if L.astrosim_abi_version() != abi.ABI_VERSION:
+        raise ImportError("libastrosim_b200.so ABI version mismatch")
+    _lib = L
+    return L
+
+
+def check(code):
+    if code != abi.OK:
+        raise AstrosimError(code, lib().astrosim_last_error().decode())
+
+
+def _u32p(a):
+    return a.ctypes.data_as(C.POINTER(C.c_uint32))
+
+
+def device_info(device=0):
+    name = C.create_string_buffer(256)
+    major, minor = C.c_int(), C.c_int()
+    check(lib().astrosim_device_info(device, name, 256, C.byref(major), C.byref(minor)))
+    return name.value.decode(), major.value, minor.value
+
+
+class Simulation:
+    """One network resident on the GPU (astrosim_create / step / summary / destroy)."""
+
+    def __init__(self, cfg=None, **overrides):
+        self.cfg = cfg if cfg is not None else default_config(**overrides)
+        self._h = C.c_void_p()
+        check(lib().astrosim_create(C.byref(self.cfg), C.byref(self._h)))
+        n_exc, n_inh, n_astro, _ = scaling(self.cfg.n_total)
+        self.n_exc, self.n_inh, self.n_astro = n_exc, n_inh, n_astro
+        self.n_neurons = n_exc + n_inh
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().astrosim_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, n):
+        check(lib().astrosim_step(self._h, int(n)))
+
+    def summary(self):
+        s = abi.Summary()
+        check(lib().astrosim_summary(self._h, C.byref(s)))
+        return s.as_dict()
+
+    def last_step_ms(self):
+        ms = C.c_double()
+        check(lib().astrosim_last_step_ms(self._h, C.byref(ms)))
+        return ms.value
+
+    def spike_counts(self, first=0, n=None):
+        if n is None:
+            n = self.summary()["steps_done"] - first
+        out = np.empty(n, dtype=np.uint32)
+        check(lib().astrosim_spike_counts(self._h, first, n, _u32p(out)))
+        return out
+
+    def raster(self):
+        words = (self.n_neurons + 31) // 32
+        steps = self.cfg.raster_steps
+        out = np.zeros(max(1, words * steps), dtype=np.uint32)
+        check(lib().astrosim_raster(self._h, _u32p(out), out.size))
+        return out[: words * steps].reshape(steps, words)
+
+    def state(self, name):
+        n = self.n_astro if name in abi.ASTRO_STATES else self.n_neurons
+        out = np.empty(n, dtype=np.float64)
+        check(lib().astrosim_get_state(self._h, abi.STATE[name], out.ctypes.data_as(C.POINTER(C.c_double)), n))
+        return out
+
+    def csr(self, name):
+        which = abi.CSR[name]
+        nt, ne = C.c_uint32(), C.c_uint64()
+        check(lib().astrosim_get_csr(self._h, which, None, 0, None, 0, C.byref(nt), C.byref(ne)))
+        rs = np.empty(nt.value + 1, dtype=np.uint32)
+        src = np.empty(max(1, ne.value), dtype=np.uint32)
+        check(lib().astrosim_get_csr(self._h, which, _u32p(rs), rs.size, _u32p(src), src.size, None, None))
+        return rs, src[: ne.value]
+
+    def dump_edges(self, path):
+        check(lib().astrosim_dump_edges(self._h, os.fsencode(path)))
+
+
+def rate_hz(spikes, n_neurons, ms):
+    return spikes / (n_neurons * ms * 1e-3) if ms > 0 else math.nan

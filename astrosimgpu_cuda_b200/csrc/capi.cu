@@ -1,0 +1,169 @@
+// capi.cu -- the extern "C" boundary declared in include/astrosim.h.
+// Every entry point converts library status into an int code and a per-thread
+// message; none of them aborts or throws across the boundary.
+
+#include <cmath>
+#include <cstring>
+#include <exception>
+#include <new>
+#include <string>
+
+#include "../../include/astrosim.h"
+#include "sim.cuh"
+
+struct astrosim_handle {
+    astrosim::Simulation sim;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int report(const astrosim::Status& s) {
+    g_last_error = s.ok() ? std::string() : s.msg;
+    return s.code;
+}
+
+int fail(int code, const char* msg) {
+    g_last_error = msg;
+    return code;
+}
+
+template <typename F>
+int guarded(F&& f) {
+    try {
+        return report(f());
+    } catch (const std::bad_alloc&) {
+        return fail(ASTROSIM_ERR_OUT_OF_MEMORY, "host allocation failed");
+    } catch (const std::exception& e) {
+        return fail(ASTROSIM_ERR_CUDA, e.what());
+    } catch (...) {
+        return fail(ASTROSIM_ERR_CUDA, "unknown exception");
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+void astrosim_config_default(astrosim_config* cfg) {
+    if (!cfg) return;
+    std::memset(cfg, 0, sizeof(*cfg));
+    cfg->struct_size = sizeof(astrosim_config);
+    cfg->n_total = 1000;      // src/astrosim_fused.cu:792-805
+    cfg->seed = 1;
+    cfg->dt = 0.1;
+    cfg->substeps = 1;
+    cfg->block = 128;
+    cfg->pre_ms = 1000.0;
+    cfg->sim_ms = 5000.0;
+    cfg->w_n2a = std::nan("");
+    cfg->w_a2n = std::nan("");
+    cfg->stp_enabled = 1;
+    cfg->precision = ASTROSIM_PRECISION_FP64;
+    cfg->neuron_drive_scale = 1.0;
+    cfg->device = 0;
+    cfg->raster_steps = 0;
+}
+
+const char* astrosim_last_error(void) { return g_last_error.c_str(); }
+
+int astrosim_abi_version(void) { return ASTROSIM_ABI_VERSION; }
+
+int astrosim_create(const astrosim_config* cfg, astrosim_handle** out) {
+    if (!cfg || !out) return fail(ASTROSIM_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    if (cfg->struct_size != sizeof(astrosim_config))
+        return fail(ASTROSIM_ERR_INVALID_ARG, "astrosim_config.struct_size mismatch (use astrosim_config_default)");
+    for (int r : cfg->reserved)
+        if (r != 0) return fail(ASTROSIM_ERR_INVALID_ARG, "astrosim_config.reserved must be zero");
+    astrosim_handle* h = nullptr;
+    try {
+        h = new astrosim_handle();
+    } catch (...) {
+        return fail(ASTROSIM_ERR_OUT_OF_MEMORY, "host allocation failed");
+    }
+    const int rc = guarded([&] { return h->sim.create(*cfg); });
+    if (rc != ASTROSIM_OK) {
+        const std::string msg = g_last_error;
+        delete h;
+        g_last_error = msg;
+        return rc;
+    }
+    *out = h;
+    return ASTROSIM_OK;
+}
+
+int astrosim_step(astrosim_handle* h, int64_t n_steps) {
+    if (!h) return fail(ASTROSIM_ERR_INVALID_ARG, "null handle");
+    return guarded([&] { return h->sim.step(n_steps); });
+}
+
+int astrosim_summary(astrosim_handle* h, astrosim_summary_t* out) {
+    if (!h || !out) return fail(ASTROSIM_ERR_INVALID_ARG, "null argument");
+    return guarded([&] { return h->sim.summary(*out); });
+}
+
+int astrosim_destroy(astrosim_handle* h) {
+    delete h;
+    g_last_error.clear();
+    return ASTROSIM_OK;
+}
+
+int astrosim_spike_counts(astrosim_handle* h, int64_t first_step, int64_t n, uint32_t* counts) {
+    if (!h) return fail(ASTROSIM_ERR_INVALID_ARG, "null handle");
+    return guarded([&] { return h->sim.spike_counts(first_step, n, counts); });
+}
+
+int astrosim_raster(astrosim_handle* h, uint32_t* bits, size_t words) {
+    if (!h) return fail(ASTROSIM_ERR_INVALID_ARG, "null handle");
+    return guarded([&] { return h->sim.raster(bits, words); });
+}
+
+int astrosim_get_state(astrosim_handle* h, int which, double* dst, size_t count) {
+    if (!h) return fail(ASTROSIM_ERR_INVALID_ARG, "null handle");
+    return guarded([&] { return h->sim.get_state(which, dst, count); });
+}
+
+int astrosim_get_csr(astrosim_handle* h, int which, uint32_t* row_start, size_t row_cap, uint32_t* src,
+                     size_t src_cap, uint32_t* n_targets, uint64_t* n_edges) {
+    if (!h) return fail(ASTROSIM_ERR_INVALID_ARG, "null handle");
+    return guarded([&] {
+        astrosim::u64 ne = 0;
+        astrosim::Status s = h->sim.get_csr(which, row_start, row_cap, src, src_cap, n_targets, &ne);
+        if (n_edges) *n_edges = ne;
+        return s;
+    });
+}
+
+int astrosim_dump_edges(astrosim_handle* h, const char* path) {
+    if (!h) return fail(ASTROSIM_ERR_INVALID_ARG, "null handle");
+    return guarded([&] { return h->sim.dump_edges(path); });
+}
+
+int astrosim_last_step_ms(astrosim_handle* h, double* ms) {
+    if (!h || !ms) return fail(ASTROSIM_ERR_INVALID_ARG, "null argument");
+    return guarded([&] { return h->sim.last_step_ms(ms); });
+}
+
+int astrosim_device_info(int device, char* name, size_t name_cap, int* major, int* minor) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return fail(ASTROSIM_ERR_NO_DEVICE, "no CUDA device visible");
+    }
+    if (device < 0 || device >= n) return fail(ASTROSIM_ERR_INVALID_ARG, "device ordinal out of range");
+    cudaDeviceProp prop{};
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess)
+        return fail(ASTROSIM_ERR_CUDA, "cudaGetDeviceProperties failed");
+    if (name && name_cap) {
+        std::strncpy(name, prop.name, name_cap - 1);
+        name[name_cap - 1] = '\0';
+    }
+    if (major) *major = prop.major;
+    if (minor) *minor = prop.minor;
+    g_last_error.clear();
+    return ASTROSIM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,109 @@
+// common.cuh -- status handling and device-memory ownership for the simulator runtime.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <utility>
+
+#include "../../include/astrosim.h"
+
+namespace astrosim {
+
+// A failed call carries a status code and a message; nothing in the library aborts.
+struct Status {
+    int code = ASTROSIM_OK;
+    std::string msg;
+    bool ok() const { return code == ASTROSIM_OK; }
+    static Status Ok() { return Status{}; }
+};
+
+inline Status make_error(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    Status s;
+    s.code = code;
+    s.msg = buf;
+    return s;
+}
+
+inline Status cuda_status(cudaError_t e, const char* what, const char* file, int line) {
+    if (e == cudaSuccess) return Status::Ok();
+    const int code = (e == cudaErrorMemoryAllocation) ? ASTROSIM_ERR_OUT_OF_MEMORY : ASTROSIM_ERR_CUDA;
+    return make_error(code, "%s failed at %s:%d: %s", what, file, line, cudaGetErrorString(e));
+}
+
+#define AS_CUDA(call)                                                                   \
+    do {                                                                                \
+        ::astrosim::Status _s = ::astrosim::cuda_status((call), #call, __FILE__, __LINE__); \
+        if (!_s.ok()) return _s;                                                        \
+    } while (0)
+
+#define AS_TRY(expr)                       \
+    do {                                   \
+        ::astrosim::Status _s = (expr);    \
+        if (!_s.ok()) return _s;           \
+    } while (0)
+
+// Owning device allocation (cudaMalloc / cudaFree), movable, never copied.
+template <typename T>
+class DevBuf {
+public:
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p_(o.p_), n_(o.n_) { o.p_ = nullptr; o.n_ = 0; }
+    DevBuf& operator=(DevBuf&& o) noexcept {
+        if (this != &o) {
+            release();
+            p_ = o.p_;
+            n_ = o.n_;
+            o.p_ = nullptr;
+            o.n_ = 0;
+        }
+        return *this;
+    }
+    ~DevBuf() { release(); }
+
+    Status alloc(size_t n) {
+        release();
+        if (n == 0) n = 1;  // keep a valid pointer for empty arrays
+        void* p = nullptr;
+        cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return make_error(ASTROSIM_ERR_OUT_OF_MEMORY, "cudaMalloc of %zu bytes failed: %s", n * sizeof(T),
+                              cudaGetErrorString(e));
+        }
+        p_ = static_cast<T*>(p);
+        n_ = n;
+        return Status::Ok();
+    }
+    Status alloc_zero(size_t n, cudaStream_t st) {
+        AS_TRY(alloc(n));
+        AS_CUDA(cudaMemsetAsync(p_, 0, n_ * sizeof(T), st));
+        return Status::Ok();
+    }
+    void release() {
+        if (p_) cudaFree(p_);
+        p_ = nullptr;
+        n_ = 0;
+    }
+    T* get() const { return p_; }
+    size_t size() const { return n_; }
+    size_t bytes() const { return n_ * sizeof(T); }
+
+private:
+    T* p_ = nullptr;
+    size_t n_ = 0;
+};
+
+inline unsigned ceil_div(uint64_t a, uint64_t b) { return static_cast<unsigned>((a + b - 1) / b); }
+
+}  // namespace astrosim

@@ -1,0 +1,243 @@
+// model.cuh -- model definition shared by every kernel of the simulator:
+// the counter RNG, the biology constants and the per-cell right-hand sides.
+//
+// The arithmetic follows the reference program (src/astrosim_fused.cu) operation
+// for operation so that results agree with it to the last bit wherever the same
+// math library is used; each function names the lines it follows.
+#pragma once
+
+#include <cmath>
+#include <cstdint>
+
+#ifndef __CUDACC__
+#define __host__
+#define __device__
+#define __forceinline__ inline
+#endif
+
+namespace astrosim {
+
+using u32 = std::uint32_t;
+using u64 = std::uint64_t;
+using i64 = std::int64_t;
+using u8 = std::uint8_t;
+using u16 = std::uint16_t;
+
+// ------------------------------------------------------------------ RNG
+// Stateless splitmix64-style hash of (seed, stream, counter):
+// src/astrosim_fused.cu:127-135.  Every random quantity in the model is a
+// pure function of these three integers, which is what lets the device
+// generate any draw of the reference's sequential streams directly.
+__host__ __device__ __forceinline__ u64 rng_bits(u64 seed, u64 stream, u64 counter) {
+    u64 z = seed;
+    z += stream * 0x9E3779B97F4A7C15ULL;
+    z += counter * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+// 53-bit uniform in [0, 1): src/astrosim_fused.cu:137-141 (double build).
+__host__ __device__ __forceinline__ double rng_uniform(u64 seed, u64 stream, u64 counter) {
+    return static_cast<double>(rng_bits(seed, stream, counter) >> 11) * (1.0 / 9007199254740992.0);
+}
+
+// True when the reference's Box-Muller redraw test (u1 <= 1e-300) rejects this draw:
+// only an all-zero top 53 bits gives a uniform that small.
+__host__ __device__ __forceinline__ bool rng_uniform_is_zero(u64 seed, u64 stream, u64 counter) {
+    return (rng_bits(seed, stream, counter) >> 11) == 0;
+}
+
+constexpr double kTwoPi = 6.283185307179586476925286766559;
+
+// Box-Muller cosine half from counters 0 and 1: src/astrosim_fused.cu:143-149.
+__host__ __device__ __forceinline__ double rng_normal(u64 seed, u64 stream) {
+    double u1 = rng_uniform(seed, stream, 0);
+    if (u1 <= 1e-300) u1 = 1e-300;
+    const double u2 = rng_uniform(seed, stream, 1);
+    return sqrt(-2.0 * log(u1)) * cos(kTwoPi * u2);
+}
+
+// Knuth's product method with a fresh (seed, stream) per draw, normal
+// approximation above lambda = 30: src/astrosim_fused.cu:154-175.
+// `limit` must be exp(-lambda); callers hoist it because lambda is a per-run constant.
+__host__ __device__ __forceinline__ int rng_poisson_knuth(u64 seed, u64 stream, double lambda, double limit) {
+    if (lambda <= 0.0) return 0;
+    if (lambda > 30.0) {
+        double u1 = rng_uniform(seed, stream, 0);
+        if (u1 <= 1e-300) u1 = 1e-300;
+        const double u2 = rng_uniform(seed, stream, 1);
+        const double z = sqrt(-2.0 * log(u1)) * cos(kTwoPi * u2);
+        const double v = lambda + sqrt(lambda) * z;
+        return v < 0.0 ? 0 : static_cast<int>(v + 0.5);
+    }
+    u64 c = 0;
+    double product = rng_uniform(seed, stream, c++);
+    int count = 0;
+    while (product > limit) {
+        ++count;
+        product *= rng_uniform(seed, stream, c++);
+    }
+    return count;
+}
+
+// Stream-selection constants of the per-step draws (src/astrosim_fused.cu:395, 404, 476, 499).
+constexpr u64 kAstroPoissonKey = 0xC2B2AE3D27D4EB4FULL;
+constexpr u64 kAstroNoiseKey = 0x9E3779B97F4A7C15ULL;
+constexpr u64 kNeuronPoissonKey = 0x2545F4914F6CDD1DULL;
+constexpr u64 kNeuronNoiseKey = 0x9E3779B185EBCA87ULL;
+constexpr u64 kCellStride = 1000003ULL;   // step * 1000003 + cell (src/astrosim_fused.cu:396, 477)
+constexpr u64 kNoiseStride = 1000033ULL;  // noise_idx * 1000033 + cell (src/astrosim_fused.cu:500)
+constexpr u64 kSetupStream = 0x5EEDULL;   // setup stream id (src/astrosim_fused.cu:634, 917)
+
+// ------------------------------------------------------------------ constants
+// Fixed-in-degree scaling law (src/astrosim_fused.cu:595-615).
+struct Sizes {
+    u32 n_total = 0, n_exc = 0, n_inh = 0, n_astro = 0, n_neurons = 0;
+    double p = 0.0;
+};
+inline Sizes scaling_law(u32 n_total) {
+    Sizes s;
+    s.n_total = n_total;
+    const long e = std::lround(n_total * 0.8);
+    s.n_exc = e < 1 ? 1u : static_cast<u32>(e);
+    s.n_inh = n_total > s.n_exc ? n_total - s.n_exc : 1u;
+    if (s.n_inh < 1) s.n_inh = 1;
+    const long a = std::lround(n_total / 5.0);
+    s.n_astro = a < 1 ? 1u : static_cast<u32>(a);
+    s.n_neurons = s.n_exc + s.n_inh;
+    const double p = 80.0 / static_cast<double>(s.n_exc);
+    s.p = p < 1.0 ? p : 1.0;
+    return s;
+}
+
+constexpr u32 kPoolSize = 5;                 // POOL_SIZE (src/astrosim_fused.cu:603)
+constexpr double kPThird = 0.2;              // P_THIRD (src/astrosim_fused.cu:600)
+constexpr u32 kMaxAstroOutDegree = 10000;    // MAX_ASTRO_OUT_DEGREE (src/astrosim_fused.cu:604)
+
+// Li-Rinzel astrocyte constants (src/astrosim_fused.cu:222-226).
+struct AstroK {
+    double Kd_IP3_1, Kd_IP3_2, Kd_act, Kd_inh, Km_SERCA;
+    double k_IP3R, rate_IP3R, rate_L, rate_SERCA, ratio_ER_cyt;
+    double SIC_scale, SIC_th;
+};
+
+// AdEx neuron constants for one population (src/astrosim_fused.cu:228-232).
+struct NeuronK {
+    double C_m, g_L, E_L, V_th, Delta_T, a, tau_w;
+    double V_peak, t_ref, E_ex, E_in, tau_syn_ex, tau_syn_in, I_e;
+    double psc_init_ex, psc_init_in;
+};
+
+// Biology defaults, compiled into the reference (src/astrosim_fused.cu:742-781).
+struct Biology {
+    double Ca_tot = 1.8958264782990153, IP3_0 = 0.010925583871830699;
+    double tau_IP3 = 1058.7589568400845, delta_IP3 = 0.04911592657233997;
+    double SIC_scale = 1.0, Kd_IP3_1 = 0.13, Kd_IP3_2 = 0.9434, Kd_act = 0.08234, Kd_inh = 1.049;
+    double Km_SERCA = 0.1, SIC_th = 0.19669, k_IP3R = 0.0002, rate_IP3R = 0.006, rate_L = 0.00011;
+    double rate_SERCA = 0.0009, ratio_ER_cyt = 0.185, Ca_init = 0.073, h_init = 0.793;
+    double IP3_init = 0.010925583871830699;
+    bool randomize_astro = true;
+    double ra_lower = 0.9, ra_upper = 1.05, ra_var = 0.1;
+
+    double e_Delta_T = 2.0, e_a = 4.0, e_tau_w = 450.0, e_V_reset = -50.0, e_b = 300.0, e_V_m = -50.0;
+    double e_C_m = 130.0, e_g_L = 18.0, e_E_L = -58.0, e_V_th = -50.0, e_V_peak = 0.0, e_t_ref = 0.0;
+    double e_E_ex = 0.0, e_E_in = -85.0, e_tau_syn_ex = 0.2, e_tau_syn_in = 2.0;
+
+    double i_Delta_T = 2.0, i_a = -0.8, i_tau_w = 264.0, i_V_reset = -60.0, i_b = 130.0, i_V_m = -60.0;
+    double i_C_m = 104.0, i_g_L = 4.3, i_E_L = -65.0, i_V_th = -52.0, i_V_peak = 0.0, i_t_ref = 0.0;
+    double i_E_ex = 0.0, i_E_in = -85.0, i_tau_syn_ex = 0.2, i_tau_syn_in = 2.0;
+
+    bool randomize_neuron = true;
+    double rn_lower = 0.9, rn_upper = 1.1, rn_var = 0.05;
+
+    double w_e = 5.0, w_i = -5.0, w_n2a = 0.2, w_a2n = 1.0;
+    double d_e = 1.0, d_i = 1.0, d_a2n = 1.0;
+    bool stp_enabled = true;
+    double stp_U = 0.5, stp_tau_rec = 800.0, stp_tau_fac = 0.0;
+    int sic_interval = 1;
+
+    double astro_poiss_rate = 3.029715502945856, astro_poiss_weight = 1.0, astro_noise_std = 0.0003;
+    double exc_poiss_rate = 2700.0, exc_poiss_weight = 1.0, exc_noise_std = 100.0;
+    double inh_poiss_rate = 2500.0, inh_poiss_weight = 1.0, inh_noise_std = 100.0;
+    bool independent_noise = true;
+    double noise_dt = 0.0;  // 0 resolves to 10 * dt (src/astrosim_fused.cu:848)
+};
+
+inline AstroK astro_constants(const Biology& b) {  // src/astrosim_fused.cu:935-938
+    AstroK k{};
+    k.Kd_IP3_1 = b.Kd_IP3_1; k.Kd_IP3_2 = b.Kd_IP3_2; k.Kd_act = b.Kd_act; k.Kd_inh = b.Kd_inh;
+    k.Km_SERCA = b.Km_SERCA; k.k_IP3R = b.k_IP3R; k.rate_IP3R = b.rate_IP3R; k.rate_L = b.rate_L;
+    k.rate_SERCA = b.rate_SERCA; k.ratio_ER_cyt = b.ratio_ER_cyt; k.SIC_scale = b.SIC_scale; k.SIC_th = b.SIC_th;
+    return k;
+}
+
+inline NeuronK neuron_constants(const Biology& b, bool exc) {  // src/astrosim_fused.cu:940-951
+    NeuronK k{};
+    k.C_m = exc ? b.e_C_m : b.i_C_m;
+    k.g_L = exc ? b.e_g_L : b.i_g_L;
+    k.E_L = exc ? b.e_E_L : b.i_E_L;
+    k.V_th = exc ? b.e_V_th : b.i_V_th;
+    k.Delta_T = exc ? b.e_Delta_T : b.i_Delta_T;
+    k.a = exc ? b.e_a : b.i_a;
+    k.tau_w = exc ? b.e_tau_w : b.i_tau_w;
+    k.V_peak = exc ? b.e_V_peak : b.i_V_peak;
+    k.t_ref = exc ? b.e_t_ref : b.i_t_ref;
+    k.E_ex = exc ? b.e_E_ex : b.i_E_ex;
+    k.E_in = exc ? b.e_E_in : b.i_E_in;
+    k.tau_syn_ex = exc ? b.e_tau_syn_ex : b.i_tau_syn_ex;
+    k.tau_syn_in = exc ? b.e_tau_syn_in : b.i_tau_syn_in;
+    k.I_e = 0.0;
+    k.psc_init_ex = 2.7182818284590452353602874713527 / k.tau_syn_ex;
+    k.psc_init_in = 2.7182818284590452353602874713527 / k.tau_syn_in;
+    return k;
+}
+
+inline int delay_to_steps(double delay_ms, double dt) {  // src/astrosim_fused.cu:783-786
+    const int s = static_cast<int>(delay_ms / dt + 0.5);
+    return s < 1 ? 1 : s;
+}
+
+// ------------------------------------------------------------------ right-hand sides
+// Li-Rinzel: src/astrosim_fused.cu:236-253 (operand order kept).
+template <typename R>
+__host__ __device__ __forceinline__ void astro_rhs(const AstroK& c, R Ca_tot, R IP3_0, R tau_IP3, R Ca, R IP3, R h,
+                                                   R noise, R& dCa, R& dIP3, R& dh) {
+    const R ratio = static_cast<R>(c.ratio_ER_cyt);
+    const R Ca_ER = (Ca_tot - Ca) / ratio;
+    const R m_inf = IP3 / (IP3 + static_cast<R>(c.Kd_IP3_1));
+    const R n_inf = Ca / (Ca + static_cast<R>(c.Kd_act));
+    const R m3 = m_inf * m_inf * m_inf;
+    const R n3 = n_inf * n_inf * n_inf;
+    const R h3 = h * h * h;
+    const R J_channel = ratio * static_cast<R>(c.rate_IP3R) * m3 * n3 * h3 * (Ca_ER - Ca);
+    const R J_pump = static_cast<R>(c.rate_SERCA) * Ca * Ca /
+                     (static_cast<R>(c.Km_SERCA) * static_cast<R>(c.Km_SERCA) + Ca * Ca);
+    const R J_leak = ratio * static_cast<R>(c.rate_L) * (Ca_ER - Ca);
+    const R alpha_h = static_cast<R>(c.k_IP3R) * static_cast<R>(c.Kd_inh) * (IP3 + static_cast<R>(c.Kd_IP3_1)) /
+                      (IP3 + static_cast<R>(c.Kd_IP3_2));
+    const R beta_h = static_cast<R>(c.k_IP3R) * Ca;
+    dCa = J_channel - J_pump + J_leak + noise;
+    dIP3 = (IP3_0 - IP3) / tau_IP3;
+    dh = alpha_h * (static_cast<R>(1.0) - h) - beta_h * h;
+}
+
+__device__ __forceinline__ double exp_r(double x) { return exp(x); }
+__device__ __forceinline__ float exp_r(float x) { return expf(x); }
+
+// AdEx: src/astrosim_fused.cu:281-290 (operand order kept).
+template <typename R>
+__device__ __forceinline__ void neuron_rhs(const NeuronK& p, R V, R w, R g_ex, R g_in, R I_ext, R& dV, R& dw) {
+    const R V_peak = static_cast<R>(p.V_peak);
+    const R Vc = V < V_peak ? V : V_peak;
+    const R I_spike = static_cast<R>(p.g_L) * static_cast<R>(p.Delta_T) *
+                      exp_r((Vc - static_cast<R>(p.V_th)) / static_cast<R>(p.Delta_T));
+    const R I_syn_ex = g_ex * (Vc - static_cast<R>(p.E_ex));
+    const R I_syn_in = g_in * (Vc - static_cast<R>(p.E_in));
+    dV = (-static_cast<R>(p.g_L) * (Vc - static_cast<R>(p.E_L)) + I_spike - I_syn_ex - I_syn_in - w +
+          static_cast<R>(p.I_e) + I_ext) /
+         static_cast<R>(p.C_m);
+    dw = (static_cast<R>(p.a) * (Vc - static_cast<R>(p.E_L)) - w) / static_cast<R>(p.tau_w);
+}
+
+}  // namespace astrosim

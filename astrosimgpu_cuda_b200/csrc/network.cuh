@@ -1,0 +1,48 @@
+// network.cuh -- the device-resident network: four target-keyed CSRs and the
+// per-cell parameters, plus the builder that makes them on the GPU.
+#pragma once
+
+#include <vector>
+
+#include "common.cuh"
+#include "model.cuh"
+
+namespace astrosim {
+
+// Target-keyed CSR (src/astrosim_fused.cu:296-301): row_start[n_targets + 1], src[n_edges].
+struct DeviceCSR {
+    DevBuf<u32> row_start, src;
+    u32 n_targets = 0;
+    u64 n_edges = 0;
+};
+
+struct Network {
+    Sizes sz;
+    u64 seed = 0;
+    DeviceCSR exc, inh, sic, e2a;
+    // Per-cell parameters (src/astrosim_fused.cu:917-933), always double.
+    DevBuf<double> Ca_tot, IP3_0, tau_IP3, delta_IP3, V_reset, b;
+    double build_seconds = 0.0;
+    int builder_path = 0;  // 0 = sequential walk, 1 = parallel chunked walk
+};
+
+struct BuildOptions {
+    // Networks whose estimated connectivity stream is shorter than this many draws are
+    // walked by one device thread (exact, no setup overhead); larger ones by the chunked
+    // parallel builder.  0 forces the parallel builder, UINT64_MAX the sequential one.
+    u64 sequential_max_draws = 4000000ULL;
+};
+
+// Builds connectivity and per-cell parameters for (sizes, seed, biology) on `stream`,
+// bit-identical in structure to the reference's host builder (src/astrosim_fused.cu:631-735)
+// and parameter draws (src/astrosim_fused.cu:917-933).
+Status build_network(const Sizes& sz, u64 seed, const Biology& bio, const BuildOptions& opt, Network& net,
+                     cudaStream_t stream);
+
+// Writes a CSR to host vectors (test and dump support).
+Status download_csr(const DeviceCSR& c, std::vector<u32>& row_start, std::vector<u32>& src, cudaStream_t st);
+
+// Expected number of setup-stream draws of the connectivity walk (for choosing the builder).
+double estimated_walk_draws(const Sizes& sz);
+
+}  // namespace astrosim

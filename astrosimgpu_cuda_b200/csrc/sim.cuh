@@ -1,0 +1,85 @@
+// sim.cuh -- one simulated network resident on the device and its time stepping.
+#pragma once
+
+#include <vector>
+
+#include "common.cuh"
+#include "model.cuh"
+#include "network.cuh"
+
+namespace astrosim {
+
+// Everything the step kernels read that does not change between steps.
+struct RunConsts {
+    AstroK ak;
+    NeuronK pe, pi;
+    double dt, h_step;
+    int substeps;
+    int d_e, d_i, d_a2n, slots;
+    int steps_per_noise;
+    int sic_interval;
+    double w_e, w_i, w_n2a, w_a2n;
+    double lambda_astro, limit_astro, weight_astro, noise_astro;
+    double lambda_exc, limit_exc, weight_exc, noise_exc;
+    double lambda_inh, limit_inh, weight_inh, noise_inh;
+    bool independent_noise;
+    bool stp_enabled;
+    double stp_U, stp_tau_rec, stp_tau_fac;
+    double SIC_th;
+    u64 seed;
+    u32 n_exc, n_neurons, n_astro, words;  // words = ceil(n_neurons / 32)
+};
+
+// Device state arrays.  V, w, Ca and IP3 are double in every precision; the
+// remaining state and the rings are `real` (double or float).
+struct StateBuffers {
+    DevBuf<double> V, w, Ca, IP3;
+    DevBuf<unsigned char> g_raw;  // g_ex, dg_ex, g_in, dg_in, I_sic, h, stp_x, stp_u as `real` (8 arrays)
+    DevBuf<double> stp_t;
+    DevBuf<int> refr;
+    DevBuf<unsigned char> ever_active;
+    DevBuf<u32> spike_bits;        // [slots][words]
+    DevBuf<unsigned char> spike_val_raw;  // [slots][n_neurons] real, written only by spiking neurons
+    DevBuf<unsigned char> sic_ring_raw;   // [slots][n_astro] real
+    DevBuf<unsigned char> sic_last_raw;   // [n_astro] real
+    DevBuf<u32> counts;            // spikes per step
+    DevBuf<u32> raster;            // [raster_steps][words]
+};
+
+class Simulation {
+public:
+    Status create(const astrosim_config& cfg);
+    Status step(i64 n);
+    Status summary(astrosim_summary_t& out);
+    Status spike_counts(i64 first, i64 n, u32* dst);
+    Status raster(u32* dst, size_t words);
+    Status get_state(int which, double* dst, size_t count);
+    Status get_csr(int which, u32* rs, size_t rs_cap, u32* src, size_t src_cap, u32* n_targets, u64* n_edges);
+    Status dump_edges(const char* path);
+    Status last_step_ms(double* ms);
+    ~Simulation();
+
+    const Sizes& sizes() const { return net_.sz; }
+    i64 steps_done() const { return steps_done_; }
+
+private:
+    Status launch_steps(i64 first, i64 count);
+    Status ensure_counts(i64 steps);
+
+    astrosim_config cfg_{};
+    Biology bio_;
+    Network net_;
+    RunConsts rc_{};
+    StateBuffers st_;
+    cudaStream_t stream_ = nullptr;
+    cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+    bool have_step_events_ = false;
+    int device_ = 0;
+    int block_ = 128;
+    bool fp32_ = false;
+    i64 pre_steps_ = 0, sim_steps_ = 0, total_steps_ = 0, steps_done_ = 0;
+    i64 counts_cap_ = 0;
+    double run_seconds_ = 0.0;
+};
+
+}  // namespace astrosim

@@ -1,0 +1,208 @@
+/*
+ * astrosim.h -- C ABI of the B200-native tripartite neuron-astrocyte simulator.
+ *
+ * The reference program (src/astrosim_fused.cu) has no library interface: it is
+ * one `main` (src/astrosim_fused.cu:791) that parses flags, builds a network on
+ * the host, steps it with two kernels per time step and prints a summary.  This
+ * header is the library boundary that replaces that monolith.  Each entry point
+ * names the part of the reference it stands in for.  All entry points:
+ *   - take plain pointers and sizes (no C++ or torch types),
+ *   - return an int status (ASTROSIM_OK == 0) and never abort the process,
+ *   - leave a human-readable message for the calling thread in
+ *     astrosim_last_error() when they fail.
+ * One handle owns one simulated network (or one ensemble) and all of its device
+ * memory; a handle must be used from one host thread at a time.
+ */
+#ifndef ASTROSIM_H
+#define ASTROSIM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ASTROSIM_ABI_VERSION 1
+
+/* Status codes. */
+enum {
+    ASTROSIM_OK = 0,
+    ASTROSIM_ERR_INVALID_ARG = 1,   /* bad pointer, size or configuration value */
+    ASTROSIM_ERR_CUDA = 2,          /* a CUDA runtime call failed */
+    ASTROSIM_ERR_OUT_OF_MEMORY = 3, /* device allocation failed */
+    ASTROSIM_ERR_UNSUPPORTED = 4,   /* configuration outside what the kernels implement */
+    ASTROSIM_ERR_NO_DEVICE = 5,     /* no CUDA device visible (reference: src/astrosim_fused.cu:906-912) */
+    ASTROSIM_ERR_TIMEOUT = 6,       /* a bounded device-side wait gave up */
+    ASTROSIM_ERR_STATE = 7,         /* call not valid in the handle's current state */
+    ASTROSIM_ERR_IO = 8             /* a host file could not be written */
+};
+
+enum {
+    ASTROSIM_PRECISION_FP64 = 0, /* every state variable and every RK4 stage in double (reference default) */
+    ASTROSIM_PRECISION_FP32 = 1  /* RK4 stages in float; V, w, Ca, IP3 accumulators and the
+                                    threshold/reset test in double */
+};
+
+/*
+ * Run configuration.  Field defaults are the reference's flag defaults
+ * (src/astrosim_fused.cu:792-805) and its compiled-in biology
+ * (src/astrosim_fused.cu:742-781).  Always initialise with
+ * astrosim_config_default() and then change fields.
+ */
+typedef struct astrosim_config {
+    uint32_t struct_size;   /* sizeof(astrosim_config); set by astrosim_config_default */
+    uint32_t n_total;       /* --n: total neurons; split by the fixed-in-degree law (src/astrosim_fused.cu:606-614) */
+    uint64_t seed;          /* --seed */
+    double dt;              /* --dt, ms */
+    int32_t substeps;       /* --substeps: RK4 substeps per time step */
+    int32_t block;          /* --block: CUDA block size for the cell kernels; 0 = autotuned choice */
+    double pre_ms;          /* --pre-ms: discarded transient */
+    double sim_ms;          /* --sim-ms: recorded window */
+    double w_n2a;           /* --w-n2a: neuron->astrocyte weight; NaN keeps the default 0.2 */
+    double w_a2n;           /* --w-a2n: astrocyte->neuron (SIC) weight; NaN keeps the default 1.0 */
+    int32_t stp_enabled;    /* 1 = Tsodyks-Markram STP on; --no-stp sets 0 */
+    int32_t precision;      /* ASTROSIM_PRECISION_FP64 or ASTROSIM_PRECISION_FP32 */
+    double neuron_drive_scale; /* multiplies the excitatory and inhibitory Poisson background rates
+                                  (2700 Hz / 2500 Hz); 1.0 reproduces the reference */
+    int32_t device;         /* CUDA device ordinal */
+    int32_t raster_steps;   /* record the full spike raster of the first raster_steps steps (0 = off) */
+    int32_t reserved[8];    /* must be zero */
+} astrosim_config;
+
+/* Result of a run, mirroring the reference's printed summary (src/astrosim_fused.cu:1103-1141). */
+typedef struct astrosim_summary_s {
+    uint32_t n_total, n_exc, n_inh, n_astro;
+    double p_primary;
+    uint64_t n_exc_edges, n_inh_edges, n_e2a_edges, n_sic_edges;
+    int64_t pre_steps, sim_steps, total_steps, steps_done;
+    uint64_t spikes_total;      /* every spike since step 0 */
+    uint64_t spikes_measured;   /* spikes in the recorded window ("spikes (recorded win)") */
+    double mean_rate_hz;        /* spikes_measured / (n_neurons * sim_ms * 1e-3) */
+    double mean_ca;             /* mean astrocyte calcium at the last completed step, uM */
+    uint32_t active_astro;      /* astrocytes with (Ca - SIC_th) * 1000 > 1 at the last step */
+    uint32_t engaged_astro;     /* astrocytes whose SIC factor was > 0 at any recorded step */
+    double sic_th;              /* SIC threshold used by the two counts above */
+    double build_seconds;       /* device connectivity + parameter build time */
+    double run_seconds;         /* wall time of the stepping since the first astrosim_step */
+} astrosim_summary_t;
+
+typedef struct astrosim_handle astrosim_handle;
+
+/* Fills *cfg with the reference defaults. */
+void astrosim_config_default(astrosim_config* cfg);
+
+/* Message describing the calling thread's most recent failure ("" if none). */
+const char* astrosim_last_error(void);
+
+/* Library ABI version (ASTROSIM_ABI_VERSION). */
+int astrosim_abi_version(void);
+
+/*
+ * Builds the network on the device and allocates its state.
+ * Replaces src/astrosim_fused.cu:846-1018: the scaling law (606-614), the host
+ * connectivity builder (631-735) and CSR inversion (304-315), the per-cell
+ * parameter draws (917-933), the initial state and the device allocations.
+ * Here every one of those steps runs on the GPU; the connectivity and the
+ * per-cell parameters are bit-identical to the reference's host code for the
+ * same (n_total, seed).
+ */
+int astrosim_create(const astrosim_config* cfg, astrosim_handle** out);
+
+/*
+ * Advances the network by n_steps time steps, asynchronously on the handle's
+ * stream.  Replaces the body of the reference time loop
+ * (src/astrosim_fused.cu:1042-1102): the per-step scalars, the astrocyte and
+ * neuron kernels, and the reset of the "engaged" flags when the pre-run ends.
+ * Steps past the configured pre+sim length are allowed.
+ */
+int astrosim_step(astrosim_handle* h, int64_t n_steps);
+
+/* Waits for the handle's stream and fills *out.  Replaces src/astrosim_fused.cu:1103-1141. */
+int astrosim_summary(astrosim_handle* h, astrosim_summary_t* out);
+
+/* Frees every device allocation the handle owns.  Accepts NULL. */
+int astrosim_destroy(astrosim_handle* h);
+
+/*
+ * Spike counts per time step for steps [first_step, first_step + n) (each
+ * step must already be done).  The reference only keeps a running total
+ * (the atomicAdd at src/astrosim_fused.cu:584) and reads it at its windowed-rate
+ * checkpoints (src/astrosim_fused.cu:1081-1095); per-step counts let a caller
+ * form those windows at any granularity.
+ */
+int astrosim_spike_counts(astrosim_handle* h, int64_t first_step, int64_t n, uint32_t* counts);
+
+/*
+ * Spike raster of the first cfg.raster_steps steps as a bitmask: bit (j % 32)
+ * of word [step * ceil(n_neurons / 32) + j / 32] is set when neuron j spiked at
+ * that step.  `words` is the capacity of `bits` in 32-bit words.
+ */
+int astrosim_raster(astrosim_handle* h, uint32_t* bits, size_t words);
+
+/* Which state array astrosim_get_state copies. */
+enum {
+    ASTROSIM_STATE_CA = 0,        /* astrocyte calcium, n_astro doubles */
+    ASTROSIM_STATE_IP3 = 1,       /* n_astro doubles */
+    ASTROSIM_STATE_H = 2,         /* IP3R gating h, n_astro doubles */
+    ASTROSIM_STATE_V = 3,         /* membrane potential, n_neurons doubles */
+    ASTROSIM_STATE_W = 4,         /* adaptation current, n_neurons doubles */
+    ASTROSIM_STATE_G_EX = 5,      /* n_neurons doubles */
+    ASTROSIM_STATE_DG_EX = 6,
+    ASTROSIM_STATE_G_IN = 7,
+    ASTROSIM_STATE_DG_IN = 8,
+    ASTROSIM_STATE_I_SIC = 9,     /* held SIC current */
+    ASTROSIM_STATE_STP_X = 10,
+    ASTROSIM_STATE_STP_U = 11,
+    ASTROSIM_STATE_STP_T_LAST = 12,
+    ASTROSIM_STATE_CA_TOT = 13,   /* per-cell parameters (src/astrosim_fused.cu:917-933) */
+    ASTROSIM_STATE_IP3_0 = 14,
+    ASTROSIM_STATE_TAU_IP3 = 15,
+    ASTROSIM_STATE_DELTA_IP3 = 16,
+    ASTROSIM_STATE_V_RESET = 17,
+    ASTROSIM_STATE_B = 18,
+    ASTROSIM_STATE_SIC_FACTOR = 19, /* astrocyte SIC factor written at the last completed step */
+    ASTROSIM_STATE_COUNT = 20
+};
+
+/* Copies one state array to host memory as doubles (count elements). */
+int astrosim_get_state(astrosim_handle* h, int which, double* dst, size_t count);
+
+/* Which connectivity CSR astrosim_get_csr copies (all keyed by TARGET, as in src/astrosim_fused.cu:296-315). */
+enum {
+    ASTROSIM_CSR_EXC = 0, /* per neuron: excitatory primary sources */
+    ASTROSIM_CSR_INH = 1, /* per neuron: inhibitory primary sources, local inhibitory indices */
+    ASTROSIM_CSR_SIC = 2, /* per neuron: astrocyte (SIC) sources */
+    ASTROSIM_CSR_E2A = 3  /* per astrocyte: excitatory third-factor sources */
+};
+
+/*
+ * Copies one CSR to host memory.  row_start receives n_targets + 1 entries,
+ * src receives n_edges entries; either may be NULL to query the sizes only.
+ */
+int astrosim_get_csr(astrosim_handle* h, int which, uint32_t* row_start, size_t row_cap,
+                     uint32_t* src, size_t src_cap, uint32_t* n_targets, uint64_t* n_edges);
+
+/*
+ * Writes the connectivity as CSV in the reference's --dump-edges format
+ * (src/astrosim_fused.cu:873-902): header "type,source,target", types
+ * exc_primary / inh_primary / n2a / a2n, inhibitory sources offset by n_exc,
+ * astrocyte ids prefixed "A".
+ */
+int astrosim_dump_edges(astrosim_handle* h, const char* path);
+
+/* Device time of the most recent astrosim_step call's kernels, ms (CUDA events, synchronises). */
+int astrosim_last_step_ms(astrosim_handle* h, double* ms);
+
+/*
+ * Name and compute capability of a CUDA device (the reference prints them after
+ * its device check, src/astrosim_fused.cu:904-914).  Returns ASTROSIM_ERR_NO_DEVICE
+ * when no device is visible.
+ */
+int astrosim_device_info(int device, char* name, size_t name_cap, int* major, int* minor);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ASTROSIM_H */
