@@ -14,6 +14,8 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
+#include <cstring>
 #include <map>
 
 #include "builder_internal.cuh"
@@ -346,7 +348,14 @@ Status build_network(const Sizes& sz, u64 seed, const Biology& bio, const BuildO
     u64 c0 = 0;
     AS_TRY(prologue_end(sz, seed, st, &c0, scratch.get()));
     const double est = estimated_walk_draws(sz);
-    if (est <= static_cast<double>(opt.sequential_max_draws)) {
+    // ASTROSIM_BUILDER=sequential|parallel forces one connectivity path (used by the
+    // tests to run both paths on the same networks).
+    u64 threshold = opt.sequential_max_draws;
+    if (const char* env = std::getenv("ASTROSIM_BUILDER")) {
+        if (std::strcmp(env, "sequential") == 0) threshold = ~0ull;
+        else if (std::strcmp(env, "parallel") == 0) threshold = 0;
+    }
+    if (est <= static_cast<double>(threshold)) {
         net.builder_path = 0;
         AS_TRY(build_sequential(sz, seed, c0, net, st));
     } else {

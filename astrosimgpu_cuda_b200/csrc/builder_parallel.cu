@@ -1,10 +1,834 @@
-// builder_parallel.cu -- chunked parallel connectivity builder (placeholder: sequential walk).
+// builder_parallel.cu -- the chunked parallel connectivity builder.
+//
+// The reference builds connectivity from ONE sequential random stream
+// (src/astrosim_fused.cu:631-723): after the pools, every presynaptic neuron
+// ("pre") walks its postsynaptic block with geometric skips, and each landing may
+// consume one or two more draws (the P_THIRD test and the pool pick).  The number
+// of draws a pre consumes depends on the draws themselves, so the tape position
+// where pre r starts is a prefix sum nobody knows in advance.  This file finds
+// every pre's start exactly, in parallel, and then emits all edges in the
+// reference's emission order:
+//
+//  1. Pools: each post's pool is 5 draws unless a duplicate forces a redraw;
+//     offsets are found by a fixed-point iteration (each round fixes at least the
+//     first misplaced post).
+//  2. Skip cache: floor(log1p(-u) / log1p(-p)) for every tape position the walks
+//     can reach, computed once; ambiguous values (quotient within a few ulps of an
+//     integer) are settled with the host C library that the reference uses.
+//  3. For each walk section (E block, I block, inhibitory pres), the section's
+//     tape is cut into chunks.  For each chunk, one CTA walks from EVERY candidate
+//     entry position in [T, T + delta) -- the chunk's first pre start must be one
+//     of them -- merging walks that land on the same pre start (a shared-memory
+//     claim table).  That gives an exact table: entry -> (exit, pres started).
+//     Tables are composed (groups in parallel, then one thread over the groups),
+//     which yields every chunk's true entry, and one thread per chunk then writes
+//     every pre's start ("orbit").
+//  4. The transfer tables ignore one index-dependent rule: in the E block a pre
+//     that lands on its own index skips its P_THIRD draws (no autapses).  Such
+//     landings are rare (about 80 per network) but shift the stream, so: every
+//     pre whose walk lands within +-K of its own index is a hazard; for each hazard
+//     a speculative exact walk from that point runs until it rejoins the table
+//     orbit; the host then replays the hazards in order with the running index
+//     shift and splices the true orbit.
+//  5. Count and emit: one thread per pre walks its row again (exact rules,
+//     including autapses), first counting, then writing edges at scanned offsets.
+//     The lists are in emission order; the stable radix sort of builder.cu turns
+//     them into the target-keyed CSRs.
+// Every step is exact; the outcome is bit-identical to the sequential walk.
+
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <vector>
+
 #include "builder_internal.cuh"
+#include "walk.cuh"
 
 namespace astrosim {
 
+namespace {
+
+constexpr u32 kHashSlots = 4096;  // per-CTA claim table (32 KB of shared memory)
+constexpr unsigned long long kEmpty = ~0ull;
+constexpr u32 kNoSelf = 0xFFFFFFFFu;
+constexpr u32 kGroup = 64;  // chunks composed per group
+constexpr u32 kMaxDelta = 512;  // candidate entries (walkers) per chunk
+
+enum ErrBits : int {
+    kErrCache = 1,     // a walk left the skip cache
+    kErrHash = 2,      // claim table full
+    kErrDelta = 4,     // an entry fell outside the candidate window
+    kErrOrbit = 8,     // materialised chunk did not meet its successor (internal)
+    kErrExplicit = 16  // re-merge walk longer than its buffer
+};
+
+struct Sec {
+    u64 seed;
+    const u32* cache;
+    u64 cache_base, cache_len;
+    int* err;
+    u32 post_count, post_off;
+    int third;
+    u32 take;
+    const u32* pool;
+};
+
+__device__ __forceinline__ u32 skip_at(const Sec& s, u64 t) {
+    const u64 i = t - s.cache_base;
+    if (i >= s.cache_len) {
+        atomicOr(s.err, kErrCache);
+        return 0xFFFFFFFFu;
+    }
+    return __ldg(s.cache + i);
+}
+
+struct NoVisit {
+    __device__ __forceinline__ void operator()(u32, bool, u32) const {}
+};
+
+// One pre's walk from tape position c (src/astrosim_fused.cu:688-707, 712-723).
+// A landing on `self_post` is an autapse: no edge and no third-factor draws.
+// Returns the tape position after the walk.
+template <class V>
+__device__ __forceinline__ u64 walk_pre(const Sec& s, u64 c, u32 self_post, V& visit) {
+    u32 pos = 0;
+    const u32 n = s.post_count;
+    while (pos < n) {
+        const u32 g = skip_at(s, c++);
+        if (g >= n - pos) break;  // the skip reaches the end of the block
+        pos += g;
+        const u32 post = s.post_off + pos;
+        ++pos;
+        if (post == self_post) continue;
+        if (s.third) {
+            const bool hit = !(rng_uniform(s.seed, kSetupStream, c++) >= kPThird);
+            u32 astro = 0;
+            if (hit) {
+                const double u = rng_uniform(s.seed, kSetupStream, c++);
+                astro = s.pool[static_cast<u64>(post) * kPoolSize +
+                               static_cast<u32>(static_cast<u64>(u * static_cast<double>(s.take)) % s.take)];
+            }
+            visit(post, hit, astro);
+        } else {
+            visit(post, false, 0u);
+        }
+    }
+    return c;
+}
+
+// ---------------------------------------------------------------- pools
+__global__ void pool_pass_kernel(u64 seed, u32 n_neurons, u32 n_astro, u32 take, u64 base, const u64* prefix,
+                                 u32* pool, u64* extra) {
+    const u32 q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n_neurons) return;
+    u64 c = base + static_cast<u64>(take) * q + prefix[q];
+    const u64 c0 = c;
+    pool_one(seed, n_astro, c, pool + static_cast<u64>(q) * kPoolSize);
+    extra[q] = c - c0 - take;
+}
+
+__global__ void diff_kernel(const u64* a, const u64* b, u64 n, int* flag) {
+    const u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n && a[i] != b[i]) *flag = 1;
+}
+
+// ---------------------------------------------------------------- skip cache
+__global__ void skip_cache_kernel(u64 seed, double L, u64 base, u64 n, u32* cache, AmbiguityLog amb) {
+    const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
+    const SkipTable none{};
+    for (u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const double g = skip_value(seed, L, base + i, none, amb);
+        cache[i] = g >= 4294967295.0 ? 0xFFFFFFFFu : static_cast<u32>(g);
+    }
+}
+
+// ---------------------------------------------------------------- chunk tables
+__global__ void table_kernel(Sec s, u64 sec_start, u32 chunk_len, u32 delta, u64* t_exit, u32* t_cnt) {
+    __shared__ unsigned long long hash[kHashSlots];
+    __shared__ int par[kMaxDelta];
+    __shared__ u32 mycnt[kMaxDelta], pcnt[kMaxDelta];
+    __shared__ unsigned long long ex[kMaxDelta];
+    for (u32 i = threadIdx.x; i < kHashSlots; i += blockDim.x) hash[i] = kEmpty;
+    __syncthreads();
+    const u64 T0 = sec_start + static_cast<u64>(blockIdx.x) * chunk_len;
+    const u64 T1 = T0 + chunk_len;
+    const u32 w = threadIdx.x;
+    if (w < delta) {
+        u64 c = T0 + w;
+        u32 cnt = 0, pc = 0;
+        int p = -1;
+        NoVisit nv;
+        while (c < T1) {
+            const u32 key = static_cast<u32>(c - T0);
+            u32 slot = (key * 2654435761u) & (kHashSlots - 1);
+            const unsigned long long mine =
+                (static_cast<unsigned long long>(key) << 32) | (static_cast<unsigned long long>(w) << 22) | cnt;
+            bool stop = false;
+            for (u32 probe = 0;; ++probe) {
+                const unsigned long long old = atomicCAS(&hash[slot], kEmpty, mine);
+                if (old == kEmpty) break;  // claimed: this walk continues from here
+                if (static_cast<u32>(old >> 32) == key) {  // another walk was here: follow it
+                    p = static_cast<int>((old >> 22) & 0x3FFu);
+                    pc = static_cast<u32>(old & 0x3FFFFFu);
+                    stop = true;
+                    break;
+                }
+                slot = (slot + 1) & (kHashSlots - 1);
+                if (probe + 1 >= kHashSlots) {
+                    atomicOr(s.err, kErrHash);
+                    stop = true;
+                    break;
+                }
+            }
+            if (stop) break;
+            c = walk_pre(s, c, kNoSelf, nv);
+            ++cnt;
+        }
+        par[w] = p;
+        mycnt[w] = cnt;
+        pcnt[w] = pc;
+        ex[w] = c;
+    }
+    __syncthreads();
+    if (w < delta) {
+        // pres from my candidate = sum over the merge chain of (mine before the merge - the
+        // claimer's count at the merge point) + the root's full count
+        long long total = 0;
+        int x = static_cast<int>(w);
+        for (u32 guard = 0; par[x] >= 0 && guard < kMaxDelta; ++guard) {
+            total += static_cast<long long>(mycnt[x]) - static_cast<long long>(pcnt[x]);
+            x = par[x];
+        }
+        total += mycnt[x];
+        t_exit[static_cast<u64>(blockIdx.x) * delta + w] = ex[x];
+        t_cnt[static_cast<u64>(blockIdx.x) * delta + w] = static_cast<u32>(total);
+    }
+}
+
+// Composes the tables of kGroup consecutive chunks: thread d follows candidate d.
+__global__ void group_compose_kernel(Sec s, u64 sec_start, u32 chunk_len, u32 delta, u32 n_chunks, const u64* t_exit,
+                                     const u32* t_cnt, u64* g_exit, u64* g_cnt) {
+    const u32 g = blockIdx.x, d = threadIdx.x;
+    if (d >= delta) return;
+    const u32 c0 = g * kGroup;
+    const u32 c1 = min(c0 + kGroup, n_chunks);
+    u64 x = d, cnt = 0, e = 0;
+    for (u32 i = c0; i < c1; ++i) {
+        if (x >= delta) {
+            atomicOr(s.err, kErrDelta);
+            break;
+        }
+        e = t_exit[static_cast<u64>(i) * delta + x];
+        cnt += t_cnt[static_cast<u64>(i) * delta + x];
+        x = e - (sec_start + static_cast<u64>(i + 1) * chunk_len);
+    }
+    g_exit[static_cast<u64>(g) * delta + d] = e;
+    g_cnt[static_cast<u64>(g) * delta + d] = cnt;
+}
+
+// One thread over the groups: the true entry and pre index of every group, up to
+// the group where `target` pres are reached.
+__global__ void top_compose_kernel(Sec s, u64 sec_start, u32 chunk_len, u32 delta, u32 n_groups, const u64* g_exit,
+                                   const u64* g_cnt, u64 target, u64* g_entry, u64* g_g0, u32* end_group) {
+    u64 e = sec_start, cnt = 0;
+    u32 g = 0;
+    for (; g < n_groups; ++g) {
+        g_entry[g] = e;
+        g_g0[g] = cnt;
+        const u64 d = e - (sec_start + static_cast<u64>(g) * kGroup * chunk_len);
+        if (d >= delta) {
+            atomicOr(s.err, kErrDelta);
+            break;
+        }
+        cnt += g_cnt[static_cast<u64>(g) * delta + d];
+        e = g_exit[static_cast<u64>(g) * delta + d];
+        if (cnt >= target) break;
+    }
+    *end_group = g;
+}
+
+// Per group: the entry and first pre index of each of its chunks.
+__global__ void chunk_entry_kernel(Sec s, u64 sec_start, u32 chunk_len, u32 delta, u32 n_chunks, u32 n_groups,
+                                   const u64* t_exit, const u32* t_cnt, const u64* g_entry, const u64* g_g0,
+                                   u64* c_entry, u64* c_g0) {
+    const u32 g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n_groups) return;
+    u64 e = g_entry[g], cnt = g_g0[g];
+    const u32 c0 = g * kGroup, c1 = min(c0 + kGroup, n_chunks);
+    for (u32 i = c0; i < c1; ++i) {
+        c_entry[i] = e;
+        c_g0[i] = cnt;
+        const u64 d = e - (sec_start + static_cast<u64>(i) * chunk_len);
+        if (d >= delta) {
+            atomicOr(s.err, kErrDelta);
+            return;
+        }
+        cnt += t_cnt[static_cast<u64>(i) * delta + d];
+        e = t_exit[static_cast<u64>(i) * delta + d];
+    }
+}
+
+// One thread per chunk writes the start of every pre that begins in the chunk.
+__global__ void materialize_kernel(Sec s, u64 sec_start, u32 chunk_len, u32 n_chunks, const u64* c_entry,
+                                   const u64* c_g0, u64 limit, u64* orbit) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_chunks) return;
+    u64 idx = c_g0[i];
+    if (idx >= limit) return;
+    const u64 T1 = sec_start + static_cast<u64>(i + 1) * chunk_len;
+    u64 c = c_entry[i];
+    NoVisit nv;
+    while (c < T1 && idx < limit) {
+        orbit[idx++] = c;
+        c = walk_pre(s, c, kNoSelf, nv);
+    }
+    if (idx < limit && i + 1 < n_chunks && c != c_entry[i + 1]) atomicOr(s.err, kErrOrbit);
+}
+
+// ---------------------------------------------------------------- autapse hazards (E block)
+struct Hazard {
+    u32 r;    // index in the table orbit
+    int d;    // landing post - r
+};
+
+struct HazardVisit {
+    u32 r;
+    int K;
+    Hazard* out;
+    unsigned* n;
+    unsigned cap;
+    __device__ __forceinline__ void operator()(u32 post, bool, u32) const {
+        const long long d = static_cast<long long>(post) - static_cast<long long>(r);
+        if (d >= -K && d <= K) {
+            const unsigned k = atomicAdd(n, 1u);
+            if (k < cap) out[k] = Hazard{r, static_cast<int>(d)};
+        }
+    }
+};
+
+__global__ void hazard_kernel(Sec s, const u64* orbit, u64 n, int K, Hazard* out, unsigned* count, unsigned cap) {
+    const u64 r = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    HazardVisit v{static_cast<u32>(r), K, out, count, cap};
+    walk_pre(s, orbit[r], kNoSelf, v);
+}
+
+struct Remerge {
+    long long k;       // table-orbit index where the exact walk rejoins (-1: section ended first)
+    long long shift;   // true index - table index after rejoining
+    u32 m;             // explicit pre starts recorded
+    u32 ok;
+    u64 end;           // section end when the walk reached the last pre
+};
+
+__device__ __forceinline__ long long find_in_orbit(const u64* orbit, u64 n, u64 c) {
+    u64 lo = 0, hi = n;
+    while (lo < hi) {
+        const u64 mid = (lo + hi) >> 1;
+        if (orbit[mid] < c) lo = mid + 1; else hi = mid;
+    }
+    return (lo < n && orbit[lo] == c) ? static_cast<long long>(lo) : -1;
+}
+
+// For each hazard, assume it is real (true index = r + d) and walk exactly from
+// there, applying the autapse rule with true indices, until the walk lands on a
+// start of the table orbit (or the section's last pre ends).
+__global__ void remerge_kernel(Sec s, const Hazard* hz, u32 n_hz, const u64* orbit, u64 n_orbit, u64 n_pres,
+                               u32 max_explicit, u64* expl, Remerge* res) {
+    const u32 h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= n_hz) return;
+    Remerge out{-1, 0, 0, 0, 0};
+    long long r = static_cast<long long>(hz[h].r) + hz[h].d;
+    if (r < 0 || r >= static_cast<long long>(n_pres)) {
+        res[h] = out;
+        return;
+    }
+    u64 c = orbit[hz[h].r];
+    u64* mine = expl + static_cast<u64>(h) * max_explicit;
+    mine[out.m++] = c;
+    NoVisit nv;
+    for (;;) {
+        c = walk_pre(s, c, static_cast<u32>(r), nv);
+        ++r;
+        if (r >= static_cast<long long>(n_pres)) {
+            out.end = c;
+            out.ok = 1;
+            break;
+        }
+        const long long k = find_in_orbit(orbit, n_orbit, c);
+        if (k >= 0) {
+            out.k = k;
+            out.shift = r - k;
+            out.ok = 1;
+            break;
+        }
+        if (out.m >= max_explicit) {
+            atomicOr(s.err, kErrExplicit);
+            break;
+        }
+        mine[out.m++] = c;
+    }
+    res[h] = out;
+}
+
+__global__ void copy_orbit_kernel(const u64* src, u64* dst, u64 n) {
+    const u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = src[i];
+}
+
+// ---------------------------------------------------------------- count and emit
+struct CountVisit {
+    u64 ne = 0, nt = 0;
+    __device__ __forceinline__ void operator()(u32, bool hit, u32) {
+        ++ne;
+        nt += hit ? 1u : 0u;
+    }
+};
+
+__device__ __forceinline__ u32 self_post_of(int mode, u32 r, u32 self_off) {
+    return mode == 0 ? kNoSelf : r + self_off;  // mode 1: autapse at post == r + self_off
+}
+
+__global__ void count_kernel(Sec s, const u64* orbit, u64 n, int self_mode, u32 self_off, u64* ce, u64* ct) {
+    const u64 r = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    CountVisit v;
+    walk_pre(s, orbit[r], self_post_of(self_mode, static_cast<u32>(r), self_off), v);
+    ce[r] = v.ne;
+    ct[r] = v.nt;
+}
+
+struct EmitVisit {
+    u32 pre;
+    u32 *e_src, *e_dst, *t_src, *t_dst, *s_src, *s_dst;
+    u64 oe, ot;
+    __device__ __forceinline__ void operator()(u32 post, bool hit, u32 astro) {
+        e_src[oe] = pre;
+        e_dst[oe] = post;
+        ++oe;
+        if (hit) {
+            t_src[ot] = pre;
+            t_dst[ot] = astro;
+            s_src[ot] = astro;
+            s_dst[ot] = post;
+            ++ot;
+        }
+    }
+};
+
+__global__ void emit_kernel(Sec s, const u64* orbit, u64 n, int self_mode, u32 self_off, const u64* oe,
+                            const u64* ot, u64 base_e, u64 base_t, u32* e_src, u32* e_dst, u32* t_src, u32* t_dst,
+                            u32* s_src, u32* s_dst) {
+    const u64 r = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    EmitVisit v{static_cast<u32>(r), e_src, e_dst, t_src, t_dst, s_src, s_dst, base_e + oe[r], base_t + ot[r]};
+    walk_pre(s, orbit[r], self_post_of(self_mode, static_cast<u32>(r), self_off), v);
+}
+
+__global__ void section_end_kernel(Sec s, const u64* orbit, u64 last, int self_mode, u32 self_off, u64* end) {
+    NoVisit nv;
+    *end = walk_pre(s, orbit[last], self_post_of(self_mode, static_cast<u32>(last), self_off), nv);
+}
+
+__global__ void max_row_kernel(const u32* rs, u32 n, unsigned* mx) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) atomicMax(mx, rs[i + 1] - rs[i]);
+}
+
+// ---------------------------------------------------------------- host helpers
+Status exclusive_scan_u64(const u64* in, u64* out, u64 n, cudaStream_t st) {
+    size_t bytes = 0;
+    AS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, st));
+    DevBuf<unsigned char> tmp;
+    AS_TRY(tmp.alloc(bytes));
+    AS_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, in, out, n, st));
+    return Status::Ok();
+}
+
+template <typename T>
+Status to_host(T* dst, const T* src, size_t n, cudaStream_t st) {
+    AS_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyDeviceToHost, st));
+    AS_CUDA(cudaStreamSynchronize(st));
+    return Status::Ok();
+}
+
+Status read_err(const DevBuf<int>& err, int* out, cudaStream_t st) { return to_host(out, err.get(), 1, st); }
+
+struct SectionPlan {
+    const char* name;
+    u32 post_count, post_off;
+    int third;
+    u64 n_pres;
+    double draws_per_pre;
+    u32 chunk_len, delta;
+    int self_mode;  // 0: no autapse possible; 1: autapse at post == r + self_off
+    u32 self_off;
+    bool autapse_shifts_stream;
+};
+
+// Finds the start of every pre of one section (steps 3 and 4 of the file comment).
+// On success `orbit` holds n_pres starts and *end the tape position after the section.
+Status section_orbit(const SectionPlan& P, Sec s, u64 start, DevBuf<int>& err, DevBuf<u64>& orbit, u64* end,
+                     cudaStream_t st) {
+    u32 chunk_len = P.chunk_len, delta = P.delta;
+    double slack = 1.04;
+    int K = 32;
+    for (int attempt = 0; attempt < 8; ++attempt) {
+        AS_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(int), st));
+        const u64 margin = P.autapse_shifts_stream ? static_cast<u64>(K) + 16 : 0;
+        const u64 target = P.n_pres + margin;
+        const double est = static_cast<double>(target) * P.draws_per_pre * slack + 8.0 * chunk_len;
+        const u32 n_chunks = std::max<u32>(1, static_cast<u32>(est / chunk_len) + 1);
+        const u32 n_groups = ceil_div(n_chunks, kGroup);
+        DevBuf<u64> t_exit, g_exit, g_cnt, g_entry, g_g0, c_entry, c_g0;
+        DevBuf<u32> t_cnt, endg;
+        AS_TRY(t_exit.alloc(static_cast<u64>(n_chunks) * delta));
+        AS_TRY(t_cnt.alloc(static_cast<u64>(n_chunks) * delta));
+        AS_TRY(g_exit.alloc(static_cast<u64>(n_groups) * delta));
+        AS_TRY(g_cnt.alloc(static_cast<u64>(n_groups) * delta));
+        AS_TRY(g_entry.alloc(n_groups));
+        AS_TRY(g_g0.alloc(n_groups));
+        AS_TRY(c_entry.alloc(n_chunks));
+        AS_TRY(c_g0.alloc(n_chunks));
+        AS_TRY(endg.alloc(1));
+        table_kernel<<<n_chunks, delta, 0, st>>>(s, start, chunk_len, delta, t_exit.get(), t_cnt.get());
+        AS_CUDA(cudaGetLastError());
+        group_compose_kernel<<<n_groups, delta, 0, st>>>(s, start, chunk_len, delta, n_chunks, t_exit.get(),
+                                                         t_cnt.get(), g_exit.get(), g_cnt.get());
+        AS_CUDA(cudaGetLastError());
+        top_compose_kernel<<<1, 1, 0, st>>>(s, start, chunk_len, delta, n_groups, g_exit.get(), g_cnt.get(), target,
+                                            g_entry.get(), g_g0.get(), endg.get());
+        AS_CUDA(cudaGetLastError());
+        int herr = 0;
+        u32 hend = 0;
+        AS_TRY(read_err(err, &herr, st));
+        AS_TRY(to_host(&hend, endg.get(), 1, st));
+        if (herr & kErrHash) { chunk_len /= 2; continue; }
+        if (herr & kErrDelta) {
+            if (delta >= kMaxDelta) return make_error(ASTROSIM_ERR_UNSUPPORTED, "%s: a pre longer than %u draws", P.name, kMaxDelta);
+            delta = std::min<u32>(kMaxDelta, delta * 2);
+            continue;
+        }
+        if (herr & kErrCache) return make_error(ASTROSIM_ERR_UNSUPPORTED, "%s walk left the skip cache", P.name);
+        if (hend >= n_groups) { slack *= 1.25; continue; }
+        const u32 used_groups = hend + 1;
+        const u32 used_chunks = std::min<u32>(n_chunks, used_groups * kGroup);
+        // sentinel entries: a chunk left unset would start past every chunk end and write nothing
+        AS_CUDA(cudaMemsetAsync(c_entry.get(), 0xFF, c_entry.bytes(), st));
+        AS_CUDA(cudaMemsetAsync(c_g0.get(), 0xFF, c_g0.bytes(), st));
+        chunk_entry_kernel<<<ceil_div(used_groups, 128), 128, 0, st>>>(s, start, chunk_len, delta, n_chunks,
+                                                                       used_groups, t_exit.get(), t_cnt.get(),
+                                                                       g_entry.get(), g_g0.get(), c_entry.get(),
+                                                                       c_g0.get());
+        AS_CUDA(cudaGetLastError());
+        AS_TRY(read_err(err, &herr, st));
+        if (herr & kErrDelta) {
+            if (delta >= kMaxDelta) return make_error(ASTROSIM_ERR_UNSUPPORTED, "%s: a pre longer than %u draws", P.name, kMaxDelta);
+            delta = std::min<u32>(kMaxDelta, delta * 2);
+            continue;
+        }
+        DevBuf<u64> forbit;
+        AS_TRY(forbit.alloc(target));
+        materialize_kernel<<<ceil_div(used_chunks, 128), 128, 0, st>>>(s, start, chunk_len, used_chunks,
+                                                                       c_entry.get(), c_g0.get(), target,
+                                                                       forbit.get());
+        AS_CUDA(cudaGetLastError());
+        AS_TRY(read_err(err, &herr, st));
+        if (herr & kErrDelta) {
+            if (delta >= kMaxDelta) return make_error(ASTROSIM_ERR_UNSUPPORTED, "%s: a pre longer than %u draws", P.name, kMaxDelta);
+            delta = std::min<u32>(kMaxDelta, delta * 2);
+            continue;
+        }
+        if (herr) return make_error(ASTROSIM_ERR_CUDA, "%s orbit materialisation failed (flags %d)", P.name, herr);
+
+        if (!P.autapse_shifts_stream) {
+            orbit = std::move(forbit);
+            DevBuf<u64> e;
+            AS_TRY(e.alloc(1));
+            section_end_kernel<<<1, 1, 0, st>>>(s, orbit.get(), P.n_pres - 1, P.self_mode, P.self_off, e.get());
+            AS_CUDA(cudaGetLastError());
+            AS_TRY(to_host(end, e.get(), 1, st));
+            return Status::Ok();
+        }
+
+        // ---- autapses of the E block (step 4)
+        const unsigned hz_cap = static_cast<unsigned>(std::min<double>(4e6, 200.0 * (2 * K + 1) + 4096));
+        DevBuf<Hazard> hz;
+        DevBuf<unsigned> hz_n;
+        AS_TRY(hz.alloc(hz_cap));
+        AS_TRY(hz_n.alloc_zero(1, st));
+        hazard_kernel<<<ceil_div(target, 128), 128, 0, st>>>(s, forbit.get(), target, K, hz.get(), hz_n.get(),
+                                                             hz_cap);
+        AS_CUDA(cudaGetLastError());
+        unsigned n_hz = 0;
+        AS_TRY(to_host(&n_hz, hz_n.get(), 1, st));
+        if (n_hz > hz_cap)
+            return make_error(ASTROSIM_ERR_UNSUPPORTED, "%s: %u autapse hazards exceed the buffer", P.name, n_hz);
+        std::vector<Hazard> hh(n_hz);
+        if (n_hz) AS_TRY(to_host(hh.data(), hz.get(), n_hz, st));
+        std::sort(hh.begin(), hh.end(), [](const Hazard& a, const Hazard& b) {
+            return a.r != b.r ? a.r < b.r : a.d < b.d;
+        });
+        // speculative exact walks from every hazard
+        const u32 max_explicit = 8192;
+        DevBuf<Hazard> hz_sorted;
+        DevBuf<Remerge> rm;
+        DevBuf<u64> expl;
+        AS_TRY(hz_sorted.alloc(std::max<unsigned>(1, n_hz)));
+        AS_TRY(rm.alloc(std::max<unsigned>(1, n_hz)));
+        AS_TRY(expl.alloc(static_cast<u64>(std::max<unsigned>(1, n_hz)) * max_explicit));
+        std::vector<Remerge> rr(n_hz);
+        if (n_hz) {
+            AS_CUDA(cudaMemcpyAsync(hz_sorted.get(), hh.data(), n_hz * sizeof(Hazard), cudaMemcpyHostToDevice, st));
+            remerge_kernel<<<ceil_div(n_hz, 64), 64, 0, st>>>(s, hz_sorted.get(), n_hz, forbit.get(), target, P.n_pres,
+                                                             max_explicit, expl.get(), rm.get());
+            AS_CUDA(cudaGetLastError());
+            AS_TRY(to_host(rr.data(), rm.get(), n_hz, st));
+            AS_TRY(read_err(err, &herr, st));
+            if (herr) return make_error(ASTROSIM_ERR_UNSUPPORTED, "%s: re-merge walks failed (flags %d)", P.name, herr);
+        }
+        // replay the hazards in order with the running shift (true index - table index)
+        struct Piece { bool expl; u64 t_start, src, len; };
+        std::vector<Piece> pieces;
+        long long d = 0;
+        u64 cur_f = 0, cur_t = 0;
+        bool ended = false;
+        u64 end_pos = 0;
+        bool shift_overflow = false;
+        for (unsigned i = 0; i < n_hz && !ended; ++i) {
+            const Hazard& h = hh[i];
+            if (h.r < cur_f || h.d != d) continue;
+            if (static_cast<long long>(h.r) + d >= static_cast<long long>(P.n_pres)) break;  // past the section
+            const Remerge& m = rr[i];
+            if (!m.ok) return make_error(ASTROSIM_ERR_CUDA, "%s: re-merge walk incomplete", P.name);
+            if (h.r > cur_f) pieces.push_back(Piece{false, cur_t, cur_f, h.r - cur_f});
+            const u64 t_autapse = static_cast<u64>(static_cast<long long>(h.r) + d);
+            pieces.push_back(Piece{true, t_autapse, static_cast<u64>(i) * max_explicit, m.m});
+            if (m.k < 0) {
+                ended = true;
+                end_pos = m.end;
+                cur_t = t_autapse + m.m;
+                break;
+            }
+            cur_t = t_autapse + m.m;
+            cur_f = static_cast<u64>(m.k);
+            d = m.shift;
+            if (d < -K || d > K) { shift_overflow = true; break; }
+        }
+        if (shift_overflow) { K *= 4; continue; }
+        if (!ended) {
+            const u64 len = P.n_pres - cur_t;
+            if (cur_f + len > target) { K *= 4; continue; }  // needed table orbit beyond the margin
+            if (len) pieces.push_back(Piece{false, cur_t, cur_f, len});
+            cur_t += len;
+        }
+        if (cur_t != P.n_pres) return make_error(ASTROSIM_ERR_CUDA, "%s: spliced orbit has %llu of %llu pres", P.name,
+                                                 static_cast<unsigned long long>(cur_t),
+                                                 static_cast<unsigned long long>(P.n_pres));
+        AS_TRY(orbit.alloc(P.n_pres));
+        for (const Piece& pc : pieces) {
+            const u64* src = pc.expl ? expl.get() + pc.src : forbit.get() + pc.src;
+            copy_orbit_kernel<<<ceil_div(pc.len, 256), 256, 0, st>>>(src, orbit.get() + pc.t_start, pc.len);
+            AS_CUDA(cudaGetLastError());
+        }
+        if (ended) {
+            *end = end_pos;
+        } else {
+            DevBuf<u64> e;
+            AS_TRY(e.alloc(1));
+            section_end_kernel<<<1, 1, 0, st>>>(s, orbit.get(), P.n_pres - 1, P.self_mode, P.self_off, e.get());
+            AS_CUDA(cudaGetLastError());
+            AS_TRY(to_host(end, e.get(), 1, st));
+        }
+        return Status::Ok();
+    }
+    return make_error(ASTROSIM_ERR_CUDA, "%s: chunked walk did not settle", P.name);
+}
+
+}  // namespace
+
 Status build_parallel(const Sizes& sz, u64 seed, u64 c0, Network& net, cudaStream_t st) {
-    return build_sequential(sz, seed, c0, net, st);
+    if (sz.p >= 1.0 || sz.n_astro <= 20)
+        return build_sequential(sz, seed, c0, net, st);  // all-to-all networks are tiny
+    const u32 nN = sz.n_neurons, nA = sz.n_astro;
+    const u32 take = nA < kPoolSize ? nA : kPoolSize;
+    DevBuf<int> err;
+    AS_TRY(err.alloc_zero(1, st));
+
+    // ---- 1. pools
+    DevBuf<u32> pool;
+    DevBuf<u64> extra, prefix, prefix_new;
+    DevBuf<int> flag;
+    AS_TRY(pool.alloc(static_cast<u64>(nN) * kPoolSize));
+    AS_TRY(extra.alloc(nN));
+    AS_TRY(prefix.alloc_zero(nN, st));
+    AS_TRY(prefix_new.alloc(nN));
+    AS_TRY(flag.alloc(1));
+    u64 pools_end = 0;
+    for (int it = 0;; ++it) {
+        if (it > 100000) return make_error(ASTROSIM_ERR_CUDA, "pool offsets did not converge");
+        pool_pass_kernel<<<ceil_div(nN, 256), 256, 0, st>>>(seed, nN, nA, take, c0, prefix.get(), pool.get(),
+                                                            extra.get());
+        AS_CUDA(cudaGetLastError());
+        AS_TRY(exclusive_scan_u64(extra.get(), prefix_new.get(), nN, st));
+        AS_CUDA(cudaMemsetAsync(flag.get(), 0, sizeof(int), st));
+        diff_kernel<<<ceil_div(nN, 256), 256, 0, st>>>(prefix.get(), prefix_new.get(), nN, flag.get());
+        AS_CUDA(cudaGetLastError());
+        int changed = 0;
+        AS_TRY(to_host(&changed, flag.get(), 1, st));
+        if (!changed) {
+            u64 last_prefix = 0, last_extra = 0;
+            AS_TRY(to_host(&last_prefix, prefix.get() + (nN - 1), 1, st));
+            AS_TRY(to_host(&last_extra, extra.get() + (nN - 1), 1, st));
+            pools_end = c0 + static_cast<u64>(take) * nN + last_prefix + last_extra;
+            break;
+        }
+        std::swap(prefix, prefix_new);
+    }
+    extra.release();
+    prefix.release();
+    prefix_new.release();
+
+    // ---- 2. skip cache over every tape position the three sections can reach
+    const double ne = sz.n_exc, ni = sz.n_inh, nn = nN, p = sz.p;
+    SectionPlan plans[3] = {
+        {"E block", sz.n_exc, 0, 1, sz.n_exc, 1.0 + p * ne * (2.0 + kPThird), 32768, 384, 1, 0, true},
+        {"I block", sz.n_inh, sz.n_exc, 1, sz.n_exc, 1.0 + p * ni * (2.0 + kPThird), 16384, 192, 0, 0, false},
+        {"inhibitory", nN, 0, 0, sz.n_inh, 1.0 + p * nn, 16384, 192, 1, sz.n_exc, false},
+    };
+    double est_total = 0.0;
+    for (const auto& P : plans) est_total += static_cast<double>(P.n_pres) * P.draws_per_pre;
+    const u64 cache_len = static_cast<u64>(est_total * 1.12) + 64ull * 65536 + 1000000;
+    DevBuf<u32> cache;
+    AS_TRY(cache.alloc(cache_len));
+    const double L = std::log1p(-p);  // host value, as the reference computes it (src/astrosim_fused.cu:622)
+    {
+        DevBuf<u64> amb_pos;
+        DevBuf<double> amb_val;
+        DevBuf<unsigned> amb_n;
+        const unsigned amb_cap = 1u << 16;
+        AS_TRY(amb_pos.alloc(amb_cap));
+        AS_TRY(amb_val.alloc(amb_cap));
+        AS_TRY(amb_n.alloc_zero(1, st));
+        AmbiguityLog amb{amb_pos.get(), amb_val.get(), amb_n.get(), amb_cap};
+        skip_cache_kernel<<<148 * 16, 256, 0, st>>>(seed, L, pools_end, cache_len, cache.get(), amb);
+        AS_CUDA(cudaGetLastError());
+        unsigned n_amb = 0;
+        AS_TRY(to_host(&n_amb, amb_n.get(), 1, st));
+        if (n_amb > amb_cap) return make_error(ASTROSIM_ERR_UNSUPPORTED, "too many ambiguous skip draws");
+        std::vector<u64> pos(n_amb);
+        if (n_amb) AS_TRY(to_host(pos.data(), amb_pos.get(), n_amb, st));
+        for (u64 t : pos) {  // settle with the host formula
+            const double g = skip_value_host(seed, L, t);
+            const u32 v = g >= 4294967295.0 ? 0xFFFFFFFFu : static_cast<u32>(g);
+            AS_CUDA(cudaMemcpyAsync(cache.get() + (t - pools_end), &v, sizeof(u32), cudaMemcpyHostToDevice, st));
+            AS_CUDA(cudaStreamSynchronize(st));
+        }
+    }
+
+    // ---- 3-4. every pre's start, section by section
+    Sec s{};
+    s.seed = seed;
+    s.cache = cache.get();
+    s.cache_base = pools_end;
+    s.cache_len = cache_len;
+    s.err = err.get();
+    s.take = take;
+    s.pool = pool.get();
+    DevBuf<u64> orbits[3];
+    u64 start = pools_end;
+    for (int k = 0; k < 3; ++k) {
+        s.post_count = plans[k].post_count;
+        s.post_off = plans[k].post_off;
+        s.third = plans[k].third;
+        u64 end = 0;
+        AS_TRY(section_orbit(plans[k], s, start, err, orbits[k], &end, st));
+        start = end;
+    }
+
+    // ---- 5. count, scan, emit
+    DevBuf<u64> ce[3], ct[3], oe[3], ot[3];
+    u64 tot_e[3] = {0, 0, 0}, tot_t[3] = {0, 0, 0};
+    for (int k = 0; k < 3; ++k) {
+        const SectionPlan& P = plans[k];
+        s.post_count = P.post_count;
+        s.post_off = P.post_off;
+        s.third = P.third;
+        AS_TRY(ce[k].alloc(P.n_pres));
+        AS_TRY(ct[k].alloc(P.n_pres));
+        AS_TRY(oe[k].alloc(P.n_pres));
+        AS_TRY(ot[k].alloc(P.n_pres));
+        count_kernel<<<ceil_div(P.n_pres, 128), 128, 0, st>>>(s, orbits[k].get(), P.n_pres, P.self_mode, P.self_off,
+                                                             ce[k].get(), ct[k].get());
+        AS_CUDA(cudaGetLastError());
+        AS_TRY(exclusive_scan_u64(ce[k].get(), oe[k].get(), P.n_pres, st));
+        AS_TRY(exclusive_scan_u64(ct[k].get(), ot[k].get(), P.n_pres, st));
+        u64 a = 0, b = 0, c = 0, d = 0;
+        AS_TRY(to_host(&a, oe[k].get() + (P.n_pres - 1), 1, st));
+        AS_TRY(to_host(&b, ce[k].get() + (P.n_pres - 1), 1, st));
+        AS_TRY(to_host(&c, ot[k].get() + (P.n_pres - 1), 1, st));
+        AS_TRY(to_host(&d, ct[k].get() + (P.n_pres - 1), 1, st));
+        tot_e[k] = a + b;
+        tot_t[k] = c + d;
+        ce[k].release();
+        ct[k].release();
+    }
+    EdgeStorage es;
+    es.cap_exc = tot_e[0] + tot_e[1];
+    es.cap_inh = tot_e[2];
+    es.cap_third = tot_t[0] + tot_t[1];
+    AS_TRY(es.exc_src.alloc(es.cap_exc));
+    AS_TRY(es.exc_dst.alloc(es.cap_exc));
+    AS_TRY(es.inh_src.alloc(es.cap_inh));
+    AS_TRY(es.inh_dst.alloc(es.cap_inh));
+    AS_TRY(es.e2a_src.alloc(es.cap_third));
+    AS_TRY(es.e2a_dst.alloc(es.cap_third));
+    AS_TRY(es.sic_src.alloc(es.cap_third));
+    AS_TRY(es.sic_dst.alloc(es.cap_third));
+    AS_TRY(es.counts.alloc_zero(4, st));
+    for (int k = 0; k < 3; ++k) {
+        const SectionPlan& P = plans[k];
+        s.post_count = P.post_count;
+        s.post_off = P.post_off;
+        s.third = P.third;
+        const u64 base_e = k == 1 ? tot_e[0] : 0, base_t = k == 1 ? tot_t[0] : 0;
+        u32* e_src = k == 2 ? es.inh_src.get() : es.exc_src.get();
+        u32* e_dst = k == 2 ? es.inh_dst.get() : es.exc_dst.get();
+        emit_kernel<<<ceil_div(P.n_pres, 128), 128, 0, st>>>(s, orbits[k].get(), P.n_pres, P.self_mode, P.self_off,
+                                                            oe[k].get(), ot[k].get(), base_e, base_t, e_src, e_dst,
+                                                            es.e2a_src.get(), es.e2a_dst.get(), es.sic_src.get(),
+                                                            es.sic_dst.get());
+        AS_CUDA(cudaGetLastError());
+    }
+    int herr = 0;
+    AS_TRY(read_err(err, &herr, st));
+    if (herr) return make_error(ASTROSIM_ERR_CUDA, "edge emission failed (flags %d)", herr);
+    for (int k = 0; k < 3; ++k) {
+        orbits[k].release();
+        oe[k].release();
+        ot[k].release();
+    }
+    cache.release();
+    pool.release();
+    const u64 counts[3] = {es.cap_exc, es.cap_inh, es.cap_third};
+    AS_TRY(edge_lists_to_network(es.view(), counts, sz, net, st));
+
+    // The astrocyte out-degree cap (src/astrosim_fused.cu:702) drops a third-factor
+    // edge only once an astrocyte already has 10000; with at most 10000 candidates
+    // per astrocyte it never fires and the lists above are exact.
+    DevBuf<unsigned> mx;
+    AS_TRY(mx.alloc_zero(1, st));
+    max_row_kernel<<<ceil_div(nA, 256), 256, 0, st>>>(net.e2a.row_start.get(), nA, mx.get());
+    AS_CUDA(cudaGetLastError());
+    unsigned hmx = 0;
+    AS_TRY(to_host(&hmx, mx.get(), 1, st));
+    if (hmx > kMaxAstroOutDegree)
+        return make_error(ASTROSIM_ERR_UNSUPPORTED,
+                          "an astrocyte has %u third-factor candidates; the out-degree cap of %u would bind", hmx,
+                          kMaxAstroOutDegree);
+    return Status::Ok();
 }
 
 }  // namespace astrosim
