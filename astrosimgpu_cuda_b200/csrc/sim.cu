@@ -4,62 +4,19 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <vector>
 
 #include "sim.cuh"
 #include "step_kernels.cuh"
+#include "window.cuh"
 
 namespace astrosim {
 
 namespace {
 
-
-template <typename R>
-StepPtrs<R> make_ptrs(StateBuffers& s, Network& n, const RunConsts& rc, i64 raster_steps) {
-    StepPtrs<R> p{};
-    p.V = s.V.get();
-    p.w = s.w.get();
-    p.Ca = s.Ca.get();
-    p.IP3 = s.IP3.get();
-    R* base = reinterpret_cast<R*>(s.g_raw.get());
-    const u64 nN = rc.n_neurons, nA = rc.n_astro;
-    p.g_ex = base;
-    p.dg_ex = base + nN;
-    p.g_in = base + 2 * nN;
-    p.dg_in = base + 3 * nN;
-    p.I_sic = base + 4 * nN;
-    p.stp_x = base + 5 * nN;
-    p.stp_u = base + 6 * nN;
-    p.h = base + 7 * nN;  // n_astro entries
-    (void)nA;
-    p.stp_t = s.stp_t.get();
-    p.refr = s.refr.get();
-    p.ever_active = s.ever_active.get();
-    p.bits = s.spike_bits.get();
-    p.val = reinterpret_cast<R*>(s.spike_val_raw.get());
-    p.sic_ring = reinterpret_cast<R*>(s.sic_ring_raw.get());
-    p.sic_last = reinterpret_cast<R*>(s.sic_last_raw.get());
-    p.counts = s.counts.get();
-    p.raster = s.raster.get();
-    p.raster_steps = raster_steps;
-    p.Ca_tot = n.Ca_tot.get();
-    p.IP3_0 = n.IP3_0.get();
-    p.tau_IP3 = n.tau_IP3.get();
-    p.delta_IP3 = n.delta_IP3.get();
-    p.V_reset = n.V_reset.get();
-    p.b = n.b.get();
-    p.exc_rs = n.exc.row_start.get();
-    p.exc_src = n.exc.src.get();
-    p.inh_rs = n.inh.row_start.get();
-    p.inh_src = n.inh.src.get();
-    p.sic_rs = n.sic.row_start.get();
-    p.sic_src = n.sic.src.get();
-    p.e2a_rs = n.e2a.row_start.get();
-    p.e2a_src = n.e2a.src.get();
-    return p;
-}
 
 // One launch = one time step for every cell: the first `astro_blocks` blocks update
 // astrocytes, the rest update neurons.  The two populations of one step read only
@@ -136,6 +93,7 @@ Biology biology_for(const astrosim_config& cfg) {
 }  // namespace
 
 Simulation::~Simulation() {
+    delete win_;
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
     if (stream_) cudaStreamDestroy(stream_);
@@ -239,9 +197,21 @@ Status Simulation::create(const astrosim_config& cfg) {
     AS_TRY(st_.stp_t.alloc(nN));
     AS_TRY(st_.refr.alloc(nN));
     AS_TRY(st_.ever_active.alloc(nA));
-    AS_TRY(st_.spike_bits.alloc_zero(static_cast<u64>(rc.slots) * rc.words, stream_));
-    AS_TRY(st_.spike_val_raw.alloc_zero(static_cast<u64>(rc.slots) * nN * rbytes, stream_));
-    AS_TRY(st_.sic_ring_raw.alloc_zero(static_cast<u64>(rc.slots) * nA * rbytes, stream_));
+    // The windowed engine runs whenever every delay is the same D in [2, 16] steps,
+    // which holds for the model's 1 ms delays at every dt from 0.0625 to 0.5 ms;
+    // ASTROSIM_STEPPER=plain keeps the per-step path (used to cross-check the two).
+    const char* stepper = std::getenv("ASTROSIM_STEPPER");
+    windowed_ = rc.d_e == rc.d_i && rc.d_i == rc.d_a2n && rc.d_e >= 2 && rc.d_e <= kMaxWindow &&
+                rc.n_neurons < (1u << 27) &&  // spike-list entries pack the neuron id in 27 bits
+                !(stepper && std::strcmp(stepper, "plain") == 0);
+    if (!windowed_) {
+        AS_TRY(st_.spike_bits.alloc_zero(static_cast<u64>(rc.slots) * rc.words, stream_));
+        AS_TRY(st_.spike_val_raw.alloc_zero(static_cast<u64>(rc.slots) * nN * rbytes, stream_));
+        AS_TRY(st_.sic_ring_raw.alloc_zero(static_cast<u64>(rc.slots) * nA * rbytes, stream_));
+    } else {
+        win_ = new WindowState();
+        AS_TRY(window_setup(rc, net_, fp32_, *win_, stream_));
+    }
     AS_TRY(st_.sic_last_raw.alloc(nA * rbytes));
     AS_TRY(st_.raster.alloc_zero(static_cast<u64>(cfg.raster_steps) * rc.words, stream_));
     AS_TRY(ensure_counts(std::max<i64>(total_steps_, 1)));
@@ -274,6 +244,10 @@ Status Simulation::ensure_counts(i64 steps) {
 }
 
 Status Simulation::launch_steps(i64 first, i64 count) {
+    if (windowed_) {
+        const i64 mark = pre_steps_ == 0 ? 0 : pre_steps_ - 1;
+        return window_launch(rc_, st_, net_, fp32_, *win_, cfg_.raster_steps, mark, first, count, stream_, block_);
+    }
     const u32 astro_blocks = ceil_div(rc_.n_astro, block_);
     const u32 neuron_blocks = ceil_div(rc_.n_neurons, block_);
     for (i64 s = first; s < first + count; ++s) {

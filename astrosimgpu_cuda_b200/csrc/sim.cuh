@@ -7,6 +7,8 @@
 #include "model.cuh"
 #include "network.cuh"
 
+namespace astrosim { struct WindowState; }
+
 namespace astrosim {
 
 // Everything the step kernels read that does not change between steps.
@@ -80,6 +82,8 @@ private:
     i64 pre_steps_ = 0, sim_steps_ = 0, total_steps_ = 0, steps_done_ = 0;
     i64 counts_cap_ = 0;
     double run_seconds_ = 0.0;
+    bool windowed_ = false;
+    WindowState* win_ = nullptr;  // owned; set when the windowed engine runs this network
 };
 
 }  // namespace astrosim

@@ -72,13 +72,18 @@ __device__ __forceinline__ void astro_advance(const AstroK& c, double Ca_tot, do
 __device__ __forceinline__ double log_r(double x) { return log(x); }
 __device__ __forceinline__ float log_r(float x) { return logf(x); }
 
-// One astrocyte for step `step` (src/astrosim_fused.cu:374-427).
+// Register-resident state of one astrocyte.
 template <typename R>
-__device__ __forceinline__ void astro_cell_step(const RunConsts& rc, const StepPtrs<R>& p, u32 a, i64 step) {
-    const int S = rc.slots;
-    const int read_slot = static_cast<int>((step + S - rc.d_e) % S);  // the e2a delay is d_e (384)
-    const R gathered = gather_spikes<R>(p.e2a_rs, p.e2a_src, a, p.bits + static_cast<u64>(read_slot) * rc.words,
-                                        p.val + static_cast<u64>(read_slot) * rc.n_neurons);
+struct AstroRegs {
+    double Ca, IP3;
+    R h;
+    double Ca_tot, IP3_0, tau_IP3, delta_IP3;
+};
+
+// Everything astrocyte `a` does in step `step` once its delayed spike sum is known
+// (src/astrosim_fused.cu:390-417): Poisson IP3 drive, noise, RK4, SIC factor.
+template <typename R>
+__device__ __forceinline__ R astro_advance_step(const RunConsts& rc, AstroRegs<R>& s, R gathered, u32 a, i64 step) {
     R ip3_input = static_cast<R>(rc.w_n2a) * gathered;
     if (rc.lambda_astro > 0.0) {
         const int ev = rng_poisson_knuth(rc.seed ^ kAstroPoissonKey, static_cast<u64>(step) * kCellStride + a,
@@ -94,37 +99,49 @@ __device__ __forceinline__ void astro_cell_step(const RunConsts& rc, const StepP
             noise = static_cast<R>(rc.noise_astro * rng_normal(rc.seed ^ kAstroNoiseKey,
                                                                static_cast<u64>(step / rc.steps_per_noise)));
     }
-    double Ca = p.Ca[a], IP3 = p.IP3[a];
-    R h = p.h[a];
-    astro_advance<R>(rc.ak, p.Ca_tot[a], p.IP3_0[a], p.tau_IP3[a], p.delta_IP3[a], ip3_input, noise, rc.h_step,
-                     rc.substeps, Ca, IP3, h);
-    p.Ca[a] = Ca;
-    p.IP3[a] = IP3;
-    p.h[a] = h;
+    astro_advance<R>(rc.ak, s.Ca_tot, s.IP3_0, s.tau_IP3, s.delta_IP3, ip3_input, noise, rc.h_step, rc.substeps,
+                     s.Ca, s.IP3, s.h);
     // SIC factor (416-417); the threshold test runs on the double Ca in every precision
-    const double y = (Ca - rc.ak.SIC_th) * 1000.0;
+    const double y = (s.Ca - rc.ak.SIC_th) * 1000.0;
     R factor = static_cast<R>(0.0);
     if (!(y <= 1.0)) factor = static_cast<R>(rc.ak.SIC_scale) * log_r(static_cast<R>(y));
+    return factor;
+}
+
+// One astrocyte for step `step` on the per-step rings (src/astrosim_fused.cu:374-427).
+template <typename R>
+__device__ __forceinline__ void astro_cell_step(const RunConsts& rc, const StepPtrs<R>& p, u32 a, i64 step) {
+    const int S = rc.slots;
+    const int read_slot = static_cast<int>((step + S - rc.d_e) % S);  // the e2a delay is d_e (384)
+    const R gathered = gather_spikes<R>(p.e2a_rs, p.e2a_src, a, p.bits + static_cast<u64>(read_slot) * rc.words,
+                                        p.val + static_cast<u64>(read_slot) * rc.n_neurons);
+    AstroRegs<R> s{p.Ca[a], p.IP3[a], p.h[a], p.Ca_tot[a], p.IP3_0[a], p.tau_IP3[a], p.delta_IP3[a]};
+    const R factor = astro_advance_step<R>(rc, s, gathered, a, step);
+    p.Ca[a] = s.Ca;
+    p.IP3[a] = s.IP3;
+    p.h[a] = s.h;
     if (factor > static_cast<R>(0.0)) p.ever_active[a] = 1;
     p.sic_ring[static_cast<u64>(step % S) * rc.n_astro + a] = factor;
     p.sic_last[a] = factor;
 }
 
-// One neuron for step `step` (src/astrosim_fused.cu:433-587).  Returns whether it
-// spiked and the value its ring entry carries.
+// Register-resident state of one neuron.
 template <typename R>
-__device__ __forceinline__ bool neuron_cell_step(const RunConsts& rc, const StepPtrs<R>& p, u32 j, i64 step,
-                                                 bool sic_refresh, u64 noise_idx, R& out_value) {
-    const int S = rc.slots;
-    const bool excitatory = j < rc.n_exc;
-    const NeuronK& pk = excitatory ? rc.pe : rc.pi;
-    const int slot_ex = static_cast<int>((step + S - rc.d_e) % S);
-    const int slot_in = static_cast<int>((step + S - rc.d_i) % S);
-    const R exc_sum = gather_spikes<R>(p.exc_rs, p.exc_src, j, p.bits + static_cast<u64>(slot_ex) * rc.words,
-                                       p.val + static_cast<u64>(slot_ex) * rc.n_neurons);
-    // inh sources are local inhibitory indices that index the ring by global id (458-463)
-    const R inh_sum = gather_spikes<R>(p.inh_rs, p.inh_src, j, p.bits + static_cast<u64>(slot_in) * rc.words,
-                                       p.val + static_cast<u64>(slot_in) * rc.n_neurons);
+struct NeuronRegs {
+    double V, w, V_reset, b;
+    R g_ex, dg_ex, g_in, dg_in, I_sic;
+    int refr;
+};
+
+// Everything neuron j does in step `step` once its delayed sums are known
+// (src/astrosim_fused.cu:465-558): synaptic inputs, Poisson drive, SIC refresh,
+// noise, the alpha-cascade closed form and AdEx RK4 (or the refractory Euler step),
+// the spike test.  `noise` is noise_std * N(0,1) for this step when `has_noise`.
+template <typename R>
+__device__ __forceinline__ bool neuron_advance_step(const RunConsts& rc, const NeuronK& pk, bool excitatory,
+                                                    NeuronRegs<R>& n, R exc_sum, R inh_sum, bool sic_refresh,
+                                                    R sic_sum, bool has_noise, double noise, u32 j, i64 step,
+                                                    R ex_decay, R in_decay) {
     R exc_input = static_cast<R>(rc.w_e) * exc_sum;
     const R inh_input = static_cast<R>(-rc.w_i) * inh_sum;
     const double lambda = excitatory ? rc.lambda_exc : rc.lambda_inh;
@@ -133,34 +150,23 @@ __device__ __forceinline__ bool neuron_cell_step(const RunConsts& rc, const Step
                                          excitatory ? rc.limit_exc : rc.limit_inh);
         if (ev > 0) exc_input += static_cast<R>(excitatory ? rc.weight_exc : rc.weight_inh) * static_cast<R>(ev);
     }
-    if (sic_refresh) {
-        const int slot_sic = static_cast<int>((step + S - rc.d_a2n) % S);
-        const R* row = p.sic_ring + static_cast<u64>(slot_sic) * rc.n_astro;
-        R sic_sum = static_cast<R>(0.0);
-        const u32 k1 = p.sic_rs[j + 1];
-        for (u32 k = p.sic_rs[j]; k < k1; ++k) sic_sum += row[p.sic_src[k]];
-        p.I_sic[j] = static_cast<R>(rc.w_a2n) * sic_sum;
-    }
-    R I_ext = p.I_sic[j];
-    const double nstd = excitatory ? rc.noise_exc : rc.noise_inh;
-    if (nstd > 0.0 && rc.independent_noise)
-        I_ext += static_cast<R>(nstd * rng_normal(rc.seed ^ kNeuronNoiseKey, noise_idx * kNoiseStride + j));
+    if (sic_refresh) n.I_sic = static_cast<R>(rc.w_a2n) * sic_sum;
+    R I_ext = n.I_sic;
+    if (has_noise) I_ext += static_cast<R>(noise);
 
-    double V = p.V[j], w = p.w[j];
-    R g_ex = p.g_ex[j], dg_ex = p.dg_ex[j] + exc_input * static_cast<R>(pk.psc_init_ex);
-    R g_in = p.g_in[j], dg_in = p.dg_in[j] + inh_input * static_cast<R>(pk.psc_init_in);
-    int refractory = p.refr[j];
+    double V = n.V, w = n.w;
+    R g_ex = n.g_ex, dg_ex = n.dg_ex + exc_input * static_cast<R>(pk.psc_init_ex);
+    R g_in = n.g_in, dg_in = n.dg_in + inh_input * static_cast<R>(pk.psc_init_in);
+    int refractory = n.refr;
     bool spiked = false;
     const R hs = static_cast<R>(rc.h_step);
-    const R ex_decay = exp_r(-hs / static_cast<R>(pk.tau_syn_ex));
-    const R in_decay = exp_r(-hs / static_cast<R>(pk.tau_syn_in));
     for (int sub = 0; sub < rc.substeps; ++sub) {
         const R g_ex_next = ex_decay * (g_ex + hs * dg_ex);
         const R dg_ex_next = ex_decay * dg_ex;
         const R g_in_next = in_decay * (g_in + hs * dg_in);
         const R dg_in_next = in_decay * dg_in;
         if (refractory > 0) {
-            V = p.V_reset[j];
+            V = n.V_reset;
             R dV, dw;
             neuron_rhs<R>(pk, static_cast<R>(V), static_cast<R>(w), g_ex, g_in, I_ext, dV, dw);
             w += static_cast<double>(hs * dw);
@@ -187,39 +193,128 @@ __device__ __forceinline__ bool neuron_cell_step(const RunConsts& rc, const Step
         if (refractory > 0) {
             --refractory;
         } else if (V >= pk.V_peak) {  // threshold test in double
-            V = p.V_reset[j];
-            w += p.b[j];
+            V = n.V_reset;
+            w += n.b;
             refractory = static_cast<int>(pk.t_ref / rc.h_step + 0.5);
             spiked = true;
         }
     }
-    p.V[j] = V;
-    p.w[j] = w;
-    p.g_ex[j] = g_ex;
-    p.dg_ex[j] = dg_ex;
-    p.g_in[j] = g_in;
-    p.dg_in[j] = dg_in;
-    p.refr[j] = refractory;
-
-    out_value = static_cast<R>(0.0);
-    if (spiked) {  // Tsodyks-Markram update of this presynaptic neuron (564-579)
-        if (rc.stp_enabled) {
-            double x = static_cast<double>(p.stp_x[j]), u = static_cast<double>(p.stp_u[j]);
-            const double t_now = static_cast<double>(step) * rc.dt;
-            const double elapsed = t_now - p.stp_t[j];
-            const double x_decay = exp(-elapsed / rc.stp_tau_rec);
-            const double u_decay = rc.stp_tau_fac < 1e-10 ? 0.0 : exp(-elapsed / rc.stp_tau_fac);
-            x = 1.0 + (x - x * u - 1.0) * x_decay;
-            u = rc.stp_U + u * (1.0 - rc.stp_U) * u_decay;
-            p.stp_x[j] = static_cast<R>(x);
-            p.stp_u[j] = static_cast<R>(u);
-            p.stp_t[j] = t_now;
-            out_value = static_cast<R>(x * u);
-        } else {
-            out_value = static_cast<R>(1.0);
-        }
-    }
+    n.V = V;
+    n.w = w;
+    n.g_ex = g_ex;
+    n.dg_ex = dg_ex;
+    n.g_in = g_in;
+    n.dg_in = dg_in;
+    n.refr = refractory;
     return spiked;
+}
+
+// Tsodyks-Markram update of a presynaptic neuron at its spike (src/astrosim_fused.cu:564-579);
+// returns the multiplier its outgoing synapses carry.
+template <typename R>
+__device__ __forceinline__ R stp_on_spike(const RunConsts& rc, R& sx, R& su, double& st, i64 step) {
+    if (!rc.stp_enabled) return static_cast<R>(1.0);
+    double x = static_cast<double>(sx), u = static_cast<double>(su);
+    const double t_now = static_cast<double>(step) * rc.dt;
+    const double elapsed = t_now - st;
+    const double x_decay = exp(-elapsed / rc.stp_tau_rec);
+    const double u_decay = rc.stp_tau_fac < 1e-10 ? 0.0 : exp(-elapsed / rc.stp_tau_fac);
+    x = 1.0 + (x - x * u - 1.0) * x_decay;
+    u = rc.stp_U + u * (1.0 - rc.stp_U) * u_decay;
+    sx = static_cast<R>(x);
+    su = static_cast<R>(u);
+    st = t_now;
+    return static_cast<R>(x * u);
+}
+
+// One neuron for step `step` on the per-step rings (src/astrosim_fused.cu:433-587).
+// Returns whether it spiked and the value its ring entry carries.
+template <typename R>
+__device__ __forceinline__ bool neuron_cell_step(const RunConsts& rc, const StepPtrs<R>& p, u32 j, i64 step,
+                                                 bool sic_refresh, u64 noise_idx, R& out_value) {
+    const int S = rc.slots;
+    const bool excitatory = j < rc.n_exc;
+    const NeuronK& pk = excitatory ? rc.pe : rc.pi;
+    const int slot_ex = static_cast<int>((step + S - rc.d_e) % S);
+    const int slot_in = static_cast<int>((step + S - rc.d_i) % S);
+    const R exc_sum = gather_spikes<R>(p.exc_rs, p.exc_src, j, p.bits + static_cast<u64>(slot_ex) * rc.words,
+                                       p.val + static_cast<u64>(slot_ex) * rc.n_neurons);
+    // inh sources are local inhibitory indices that index the ring by global id (458-463)
+    const R inh_sum = gather_spikes<R>(p.inh_rs, p.inh_src, j, p.bits + static_cast<u64>(slot_in) * rc.words,
+                                       p.val + static_cast<u64>(slot_in) * rc.n_neurons);
+    R sic_sum = static_cast<R>(0.0);
+    if (sic_refresh) {
+        const int slot_sic = static_cast<int>((step + S - rc.d_a2n) % S);
+        const R* row = p.sic_ring + static_cast<u64>(slot_sic) * rc.n_astro;
+        const u32 k1 = p.sic_rs[j + 1];
+        for (u32 k = p.sic_rs[j]; k < k1; ++k) sic_sum += row[p.sic_src[k]];
+    }
+    const double nstd = excitatory ? rc.noise_exc : rc.noise_inh;
+    const bool has_noise = nstd > 0.0 && rc.independent_noise;
+    const double noise = has_noise ? nstd * rng_normal(rc.seed ^ kNeuronNoiseKey, noise_idx * kNoiseStride + j) : 0.0;
+    NeuronRegs<R> n{p.V[j], p.w[j], p.V_reset[j], p.b[j], p.g_ex[j], p.dg_ex[j], p.g_in[j], p.dg_in[j], p.I_sic[j],
+                    p.refr[j]};
+    const R hs = static_cast<R>(rc.h_step);
+    const R ex_decay = exp_r(-hs / static_cast<R>(pk.tau_syn_ex));
+    const R in_decay = exp_r(-hs / static_cast<R>(pk.tau_syn_in));
+    const bool spiked = neuron_advance_step<R>(rc, pk, excitatory, n, exc_sum, inh_sum, sic_refresh, sic_sum,
+                                               has_noise, noise, j, step, ex_decay, in_decay);
+    p.V[j] = n.V;
+    p.w[j] = n.w;
+    p.g_ex[j] = n.g_ex;
+    p.dg_ex[j] = n.dg_ex;
+    p.g_in[j] = n.g_in;
+    p.dg_in[j] = n.dg_in;
+    p.refr[j] = n.refr;
+    if (sic_refresh) p.I_sic[j] = n.I_sic;
+    out_value = static_cast<R>(0.0);
+    if (spiked) out_value = stp_on_spike<R>(rc, p.stp_x[j], p.stp_u[j], p.stp_t[j], step);
+    return spiked;
+}
+
+// Device pointers of a simulation's state and network (host side).
+template <typename R>
+inline StepPtrs<R> make_ptrs(StateBuffers& s, Network& n, const RunConsts& rc, i64 raster_steps) {
+    StepPtrs<R> p{};
+    p.V = s.V.get();
+    p.w = s.w.get();
+    p.Ca = s.Ca.get();
+    p.IP3 = s.IP3.get();
+    R* base = reinterpret_cast<R*>(s.g_raw.get());
+    const u64 nN = rc.n_neurons;
+    p.g_ex = base;
+    p.dg_ex = base + nN;
+    p.g_in = base + 2 * nN;
+    p.dg_in = base + 3 * nN;
+    p.I_sic = base + 4 * nN;
+    p.stp_x = base + 5 * nN;
+    p.stp_u = base + 6 * nN;
+    p.h = base + 7 * nN;  // n_astro entries
+    p.stp_t = s.stp_t.get();
+    p.refr = s.refr.get();
+    p.ever_active = s.ever_active.get();
+    p.bits = s.spike_bits.get();
+    p.val = reinterpret_cast<R*>(s.spike_val_raw.get());
+    p.sic_ring = reinterpret_cast<R*>(s.sic_ring_raw.get());
+    p.sic_last = reinterpret_cast<R*>(s.sic_last_raw.get());
+    p.counts = s.counts.get();
+    p.raster = s.raster.get();
+    p.raster_steps = raster_steps;
+    p.Ca_tot = n.Ca_tot.get();
+    p.IP3_0 = n.IP3_0.get();
+    p.tau_IP3 = n.tau_IP3.get();
+    p.delta_IP3 = n.delta_IP3.get();
+    p.V_reset = n.V_reset.get();
+    p.b = n.b.get();
+    p.exc_rs = n.exc.row_start.get();
+    p.exc_src = n.exc.src.get();
+    p.inh_rs = n.inh.row_start.get();
+    p.inh_src = n.inh.src.get();
+    p.sic_rs = n.sic.row_start.get();
+    p.sic_src = n.sic.src.get();
+    p.e2a_rs = n.e2a.row_start.get();
+    p.e2a_src = n.e2a.src.get();
+    return p;
 }
 
 }  // namespace astrosim

@@ -1,0 +1,444 @@
+// window.cu -- windowed stepping: one launch per window of D steps plus one push
+// launch between windows (see window.cuh).
+
+#include <cub/device/device_radix_sort.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+
+#include "step_kernels.cuh"
+#include "window.cuh"
+
+namespace astrosim {
+
+namespace {
+
+template <typename R>
+struct WinPtrs {
+    u32 *nin_cnt, *ain_cnt;          // [2][n]
+    Deposit<R> *nin_ent, *ain_ent;   // [2][n][kInboxSlots]
+    u32* spk_word;                   // [2][n_neurons]
+    R* spk_val;                      // [2][W][n_neurons]
+    u32* spk_list;                   // [2][cap]
+    u32* spk_count;                  // [2]
+    R* sic_win;                      // [2][n_astro][W]
+    u32* astro_active;               // [2][astro_words]
+    int* mode;                       // [2]
+    const u32 *fe_rs, *fe_dst, *fi_rs, *fi_dst, *fa_rs, *fa_astro, *fa_pos;
+    u32 cap, push_limit, astro_words;
+    int W;
+};
+
+template <typename R>
+WinPtrs<R> win_ptrs(WindowState& ws, const RunConsts& rc) {
+    WinPtrs<R> w{};
+    w.nin_cnt = ws.nin_cnt.get();
+    w.ain_cnt = ws.ain_cnt.get();
+    w.nin_ent = reinterpret_cast<Deposit<R>*>(ws.nin_ent.get());
+    w.ain_ent = reinterpret_cast<Deposit<R>*>(ws.ain_ent.get());
+    w.spk_word = ws.spk_word.get();
+    w.spk_val = reinterpret_cast<R*>(ws.spk_val.get());
+    w.spk_list = ws.spk_list.get();
+    w.spk_count = ws.spk_count.get();
+    w.sic_win = reinterpret_cast<R*>(ws.sic_win.get());
+    w.astro_active = ws.astro_active.get();
+    w.mode = ws.mode.get();
+    w.fe_rs = ws.fwd.exc_rs.get();
+    w.fe_dst = ws.fwd.exc_dst.get();
+    w.fi_rs = ws.fwd.inh_rs.get();
+    w.fi_dst = ws.fwd.inh_dst.get();
+    w.fa_rs = ws.fwd.e2a_rs.get();
+    w.fa_astro = ws.fwd.e2a_astro.get();
+    w.fa_pos = ws.fwd.e2a_pos.get();
+    w.cap = ws.push_limit + 1;
+    w.push_limit = ws.push_limit;
+    w.astro_words = (rc.n_astro + 31) / 32;
+    w.W = ws.W;
+    return w;
+}
+
+// Sorts deposits by (step, kind, key): the order in which the reference's dense
+// gather meets them (row order within one step and kind).
+template <typename R>
+__device__ __forceinline__ void sort_deposits(Deposit<R>* d, int n) {
+    for (int i = 1; i < n; ++i) {
+        const Deposit<R> x = d[i];
+        const unsigned long long kx = (static_cast<unsigned long long>(x.meta) << 32) | x.key;
+        int k = i - 1;
+        while (k >= 0 && ((static_cast<unsigned long long>(d[k].meta) << 32) | d[k].key) > kx) {
+            d[k + 1] = d[k];
+            --k;
+        }
+        d[k + 1] = x;
+    }
+}
+
+// Per-step sums of one CSR row against the previous window's spike words, in row
+// order (the exact fallback when deposits are not available).
+template <typename R>
+__device__ __forceinline__ void pull_row(const u32* __restrict__ rs, const u32* __restrict__ src, u32 row,
+                                         const u32* __restrict__ words, const R* __restrict__ vals, u64 n_neurons,
+                                         int s0, int s1, R* acc) {
+    const u32 k1 = rs[row + 1];
+    for (u32 k = rs[row]; k < k1; ++k) {
+        const u32 s = src[k];
+        u32 wd = words[s];
+        if (!wd) continue;
+        wd &= ((s1 >= 32 ? 0xFFFFFFFFu : ((1u << s1) - 1u)) & ~((1u << s0) - 1u));
+        while (wd) {
+            const int b = __ffs(wd) - 1;
+            wd &= wd - 1;
+            acc[b] += vals[static_cast<u64>(b) * n_neurons + s];
+        }
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(128) window_kernel(RunConsts rc, StepPtrs<R> p, WinPtrs<R> w, i64 win_start,
+                                                     int s_begin, int s_end, int buf, i64 mark, u32 astro_blocks) {
+    const int prev = buf ^ 1;
+    const int W = w.W;
+    const bool window_done = s_end == W;
+    const bool pull = w.mode[buf] != 0;
+    if (blockIdx.x < astro_blocks) {
+        // ------------------------------------------------------------ astrocytes
+        const u32 a = blockIdx.x * blockDim.x + threadIdx.x;
+        const bool valid = a < rc.n_astro;
+        bool any_active = false;
+        if (valid) {
+            AstroRegs<R> s{p.Ca[a], p.IP3[a], p.h[a], p.Ca_tot[a], p.IP3_0[a], p.tau_IP3[a], p.delta_IP3[a]};
+            R acc[kMaxWindow];
+            const u64 slot_base = (static_cast<u64>(buf) * rc.n_astro + a);
+            const u32 c = w.ain_cnt[slot_base];
+            const bool ip3_input = pull || c > 0;
+            if (ip3_input)
+                for (int i = 0; i < W; ++i) acc[i] = static_cast<R>(0.0);
+            if (pull || c > kInboxSlots) {
+                pull_row<R>(p.e2a_rs, p.e2a_src, a, w.spk_word + static_cast<u64>(prev) * rc.n_neurons,
+                            w.spk_val + static_cast<u64>(prev) * W * rc.n_neurons, rc.n_neurons, s_begin, s_end, acc);
+            } else if (c > 0) {
+                Deposit<R> d[kInboxSlots];
+                for (u32 i = 0; i < c; ++i) d[i] = w.ain_ent[slot_base * kInboxSlots + i];
+                sort_deposits<R>(d, static_cast<int>(c));
+                for (u32 i = 0; i < c; ++i) {
+                    const int st = static_cast<int>(d[i].meta & 0xFFu);
+                    if (st >= s_begin && st < s_end) acc[st] += d[i].val;
+                }
+            }
+            if (window_done && c) w.ain_cnt[slot_base] = 0;
+            unsigned char ever = p.ever_active[a];
+            R* out = w.sic_win + (static_cast<u64>(buf) * rc.n_astro + a) * W;
+            R factor = static_cast<R>(0.0);
+            for (int st = s_begin; st < s_end; ++st) {
+                const i64 t = win_start + st;
+                factor = astro_advance_step<R>(rc, s, ip3_input ? acc[st] : static_cast<R>(0.0), a, t);
+                out[st] = factor;
+                if (factor > static_cast<R>(0.0)) {
+                    ever = 1;
+                    any_active = true;
+                }
+                if (t == mark) ever = 0;  // end of the pre-run (src/astrosim_fused.cu:1075)
+            }
+            p.Ca[a] = s.Ca;
+            p.IP3[a] = s.IP3;
+            p.h[a] = s.h;
+            p.ever_active[a] = ever;
+            p.sic_last[a] = factor;
+        }
+        const unsigned ballot = __ballot_sync(0xffffffffu, any_active);
+        if ((threadIdx.x & 31) == 0 && a < rc.n_astro) {
+            u32* word = w.astro_active + static_cast<u64>(buf) * w.astro_words + (a >> 5);
+            if (s_begin == 0) *word = ballot; else if (ballot) atomicOr(word, ballot);
+        }
+        return;
+    }
+    // ---------------------------------------------------------------- neurons
+    const u32 j = (blockIdx.x - astro_blocks) * blockDim.x + threadIdx.x;
+    if (j >= rc.n_neurons) return;
+    const bool excitatory = j < rc.n_exc;
+    const NeuronK& pk = excitatory ? rc.pe : rc.pi;
+    const u64 nN = rc.n_neurons;
+
+    // synaptic input of the window: deposits (push) or the row walk (pull)
+    R ex_acc[kMaxWindow], in_acc[kMaxWindow];
+    const u64 slot_base = static_cast<u64>(buf) * nN + j;
+    const u32 c = w.nin_cnt[slot_base];
+    const bool syn_input = pull || c > 0;
+    if (syn_input)
+        for (int i = 0; i < W; ++i) ex_acc[i] = in_acc[i] = static_cast<R>(0.0);
+    if (pull || c > kInboxSlots) {
+        const u32* words = w.spk_word + static_cast<u64>(prev) * nN;
+        const R* vals = w.spk_val + static_cast<u64>(prev) * W * nN;
+        pull_row<R>(p.exc_rs, p.exc_src, j, words, vals, nN, s_begin, s_end, ex_acc);
+        pull_row<R>(p.inh_rs, p.inh_src, j, words, vals, nN, s_begin, s_end, in_acc);
+    } else if (c > 0) {
+        Deposit<R> d[kInboxSlots];
+        for (u32 i = 0; i < c; ++i) d[i] = w.nin_ent[slot_base * kInboxSlots + i];
+        sort_deposits<R>(d, static_cast<int>(c));
+        for (u32 i = 0; i < c; ++i) {
+            const int st = static_cast<int>(d[i].meta & 0xFFu);
+            if (st < s_begin || st >= s_end) continue;
+            if ((d[i].meta >> 8) == 0) ex_acc[st] += d[i].val; else in_acc[st] += d[i].val;
+        }
+    }
+    if (window_done && c) w.nin_cnt[slot_base] = 0;
+
+    // SIC factors of the previous window through the active-astrocyte bitmask
+    R sic_acc[kMaxWindow];
+    bool sic_input = false;
+    {
+        const u32* act = w.astro_active + static_cast<u64>(prev) * w.astro_words;
+        const R* fac = w.sic_win + static_cast<u64>(prev) * rc.n_astro * W;
+        const u32 k1 = p.sic_rs[j + 1];
+        for (u32 k = p.sic_rs[j]; k < k1; ++k) {
+            const u32 a = p.sic_src[k];
+            if (!((act[a >> 5] >> (a & 31)) & 1u)) continue;  // every factor of this astrocyte was 0
+            if (!sic_input) {
+                for (int i = 0; i < W; ++i) sic_acc[i] = static_cast<R>(0.0);
+                sic_input = true;
+            }
+            const R* f = fac + static_cast<u64>(a) * W;
+            for (int st = s_begin; st < s_end; ++st) sic_acc[st] += f[st];
+        }
+    }
+
+    NeuronRegs<R> n{p.V[j], p.w[j], p.V_reset[j], p.b[j], p.g_ex[j], p.dg_ex[j], p.g_in[j], p.dg_in[j], p.I_sic[j],
+                    p.refr[j]};
+    const R hs = static_cast<R>(rc.h_step);
+    const R ex_decay = exp_r(-hs / static_cast<R>(pk.tau_syn_ex));
+    const R in_decay = exp_r(-hs / static_cast<R>(pk.tau_syn_in));
+    const double nstd = excitatory ? rc.noise_exc : rc.noise_inh;
+    const bool has_noise = nstd > 0.0 && rc.independent_noise;
+    u64 noise_idx_cached = ~0ull;
+    double noise = 0.0;
+    u32 word = 0;
+    R* vout = w.spk_val + static_cast<u64>(buf) * W * nN;
+    for (int st = s_begin; st < s_end; ++st) {
+        const i64 t = win_start + st;
+        const bool refresh = (t - rc.d_a2n >= 0) && ((t - rc.d_a2n) % rc.sic_interval == 0);
+        if (has_noise) {
+            const u64 idx = static_cast<u64>(t / rc.steps_per_noise);
+            if (idx != noise_idx_cached) {
+                noise = nstd * rng_normal(rc.seed ^ kNeuronNoiseKey, idx * kNoiseStride + j);
+                noise_idx_cached = idx;
+            }
+        }
+        const R zero = static_cast<R>(0.0);
+        const bool spiked = neuron_advance_step<R>(
+            rc, pk, excitatory, n, syn_input ? ex_acc[st] : zero, syn_input ? in_acc[st] : zero, refresh,
+            sic_input ? sic_acc[st] : zero, has_noise, noise, j, t, ex_decay, in_decay);
+        if (spiked) {
+            const R out = stp_on_spike<R>(rc, p.stp_x[j], p.stp_u[j], p.stp_t[j], t);
+            vout[static_cast<u64>(st) * nN + j] = out;
+            word |= 1u << st;
+            const u32 slot = atomicAdd(&w.spk_count[buf], 1u);
+            if (slot < w.cap) w.spk_list[static_cast<u64>(buf) * w.cap + slot] = (j << 5) | static_cast<u32>(st);
+            atomicAdd(&p.counts[t], 1u);
+            if (t < p.raster_steps) atomicOr(&p.raster[static_cast<u64>(t) * rc.words + (j >> 5)], 1u << (j & 31));
+        }
+    }
+    p.V[j] = n.V;
+    p.w[j] = n.w;
+    p.g_ex[j] = n.g_ex;
+    p.dg_ex[j] = n.dg_ex;
+    p.g_in[j] = n.g_in;
+    p.dg_in[j] = n.dg_in;
+    p.I_sic[j] = n.I_sic;
+    p.refr[j] = n.refr;
+    u32* sw = w.spk_word + slot_base;
+    *sw = s_begin == 0 ? word : (*sw | word);
+}
+
+// After window `buf` completes: deliver its spikes into the inboxes of the next
+// window (buffer buf ^ 1), or switch the next window to pull when it was busy.
+template <typename R>
+__global__ void push_kernel(WinPtrs<R> w, u32 n_exc, u32 n_inh, u64 n_neurons, u64 n_astro, int buf) {
+    const int nxt = buf ^ 1;
+    const u32 n = w.spk_count[buf];
+    const bool busy = n > w.push_limit;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        w.mode[nxt] = busy ? 1 : 0;
+        w.spk_count[nxt] = 0;  // the next window appends its spikes there
+    }
+    if (busy) return;
+    const u32 lane = threadIdx.x & 31;
+    const u64 warp = (static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const u64 n_warps = (static_cast<u64>(gridDim.x) * blockDim.x) >> 5;
+    const R* vals = w.spk_val + static_cast<u64>(buf) * w.W * n_neurons;
+    for (u64 e = warp; e < n; e += n_warps) {
+        const u32 packed = w.spk_list[static_cast<u64>(buf) * w.cap + e];
+        const u32 j = packed >> 5, st = packed & 31u;
+        const R v = vals[static_cast<u64>(st) * n_neurons + j];
+        if (j < n_exc) {
+            for (u32 k = w.fe_rs[j] + lane; k < w.fe_rs[j + 1]; k += 32) {
+                const u32 t = w.fe_dst[k];
+                const u64 sb = static_cast<u64>(nxt) * n_neurons + t;
+                const u32 slot = atomicAdd(&w.nin_cnt[sb], 1u);
+                if (slot < kInboxSlots) w.nin_ent[sb * kInboxSlots + slot] = Deposit<R>{j, st, v};
+            }
+            for (u32 k = w.fa_rs[j] + lane; k < w.fa_rs[j + 1]; k += 32) {
+                const u32 a = w.fa_astro[k];
+                const u64 sb = static_cast<u64>(nxt) * n_astro + a;
+                const u32 slot = atomicAdd(&w.ain_cnt[sb], 1u);
+                if (slot < kInboxSlots) w.ain_ent[sb * kInboxSlots + slot] = Deposit<R>{w.fa_pos[k], st, v};
+            }
+        }
+        // the inhibitory rows hold local inhibitory ids and read the spike ring by
+        // global id (src/astrosim_fused.cu:458-463): neuron j feeds them when j < n_inh
+        if (j < n_inh) {
+            for (u32 k = w.fi_rs[j] + lane; k < w.fi_rs[j + 1]; k += 32) {
+                const u32 t = w.fi_dst[k];
+                const u64 sb = static_cast<u64>(nxt) * n_neurons + t;
+                const u32 slot = atomicAdd(&w.nin_cnt[sb], 1u);
+                if (slot < kInboxSlots) w.nin_ent[sb * kInboxSlots + slot] = Deposit<R>{j, st | (1u << 8), v};
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------ forward CSRs
+__global__ void edge_rows_kernel(const u32* rs, u32 n_rows, u32* row_of_edge) {
+    const u32 r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n_rows) return;
+    for (u32 k = rs[r]; k < rs[r + 1]; ++k) row_of_edge[k] = r;
+}
+
+__global__ void iota_kernel(u32* v, u64 n) {
+    const u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = static_cast<u32>(i);
+}
+
+__global__ void lower_bound_rows_kernel(const u32* sorted_keys, u64 n, u32 n_rows, u32* rs) {
+    const u64 t = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t > n_rows) return;
+    u64 lo = 0, hi = n;
+    while (lo < hi) {
+        const u64 mid = (lo + hi) >> 1;
+        if (sorted_keys[mid] < t) lo = mid + 1; else hi = mid;
+    }
+    rs[t] = static_cast<u32>(lo);
+}
+
+__global__ void gather_fwd_kernel(const u32* edge_idx, u64 n, const u32* row_of_edge, const u32* tgt_rs, u32* dst,
+                                  u32* pos) {
+    const u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const u32 e = edge_idx[i];
+    const u32 r = row_of_edge[e];
+    dst[i] = r;
+    if (pos) pos[i] = e - tgt_rs[r];
+}
+
+__global__ void max_fanout_kernel(const u32* rs, u32 n, unsigned* mx) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) atomicMax(mx, rs[i + 1] - rs[i]);
+}
+
+// Inverts a target-keyed CSR into a source-keyed one.  Within one source the
+// targets come out in increasing edge order (stable sort), which the push does not
+// depend on; positions let e2a deposits name their place in the target row.
+Status invert_csr(const DeviceCSR& c, u32 n_sources, DevBuf<u32>& rs, DevBuf<u32>& dst, DevBuf<u32>* pos,
+                  cudaStream_t st) {
+    const u64 n = c.n_edges;
+    AS_TRY(rs.alloc(static_cast<size_t>(n_sources) + 1));
+    AS_TRY(dst.alloc(n));
+    if (pos) AS_TRY(pos->alloc(n));
+    if (n == 0) {
+        AS_CUDA(cudaMemsetAsync(rs.get(), 0, rs.bytes(), st));
+        return Status::Ok();
+    }
+    DevBuf<u32> row_of, idx_in, keys_out, idx_out;
+    AS_TRY(row_of.alloc(n));
+    AS_TRY(idx_in.alloc(n));
+    AS_TRY(keys_out.alloc(n));
+    AS_TRY(idx_out.alloc(n));
+    edge_rows_kernel<<<ceil_div(c.n_targets, 256), 256, 0, st>>>(c.row_start.get(), c.n_targets, row_of.get());
+    iota_kernel<<<ceil_div(n, 256), 256, 0, st>>>(idx_in.get(), n);
+    AS_CUDA(cudaGetLastError());
+    int end_bit = 1;
+    while (end_bit < 32 && (1ull << end_bit) < static_cast<u64>(n_sources) + 1) ++end_bit;
+    size_t tb = 0;
+    AS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, c.src.get(), keys_out.get(), idx_in.get(), idx_out.get(), n,
+                                            0, end_bit, st));
+    DevBuf<unsigned char> tmp;
+    AS_TRY(tmp.alloc(tb));
+    AS_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), tb, c.src.get(), keys_out.get(), idx_in.get(), idx_out.get(), n,
+                                            0, end_bit, st));
+    lower_bound_rows_kernel<<<ceil_div(static_cast<u64>(n_sources) + 1, 256), 256, 0, st>>>(keys_out.get(), n,
+                                                                                          n_sources, rs.get());
+    gather_fwd_kernel<<<ceil_div(n, 256), 256, 0, st>>>(idx_out.get(), n, row_of.get(), c.row_start.get(), dst.get(),
+                                                        pos ? pos->get() : nullptr);
+    AS_CUDA(cudaGetLastError());
+    AS_CUDA(cudaStreamSynchronize(st));
+    return Status::Ok();
+}
+
+}  // namespace
+
+Status window_setup(const RunConsts& rc, Network& net, bool fp32, WindowState& ws, cudaStream_t st) {
+    ws.W = rc.d_e;
+    const u64 nN = rc.n_neurons, nA = rc.n_astro;
+    const size_t rb = fp32 ? sizeof(float) : sizeof(double);
+    const size_t db = fp32 ? sizeof(Deposit<float>) : sizeof(Deposit<double>);
+    AS_TRY(invert_csr(net.exc, rc.n_exc, ws.fwd.exc_rs, ws.fwd.exc_dst, nullptr, st));
+    AS_TRY(invert_csr(net.inh, net.sz.n_inh, ws.fwd.inh_rs, ws.fwd.inh_dst, nullptr, st));
+    AS_TRY(invert_csr(net.e2a, rc.n_exc, ws.fwd.e2a_rs, ws.fwd.e2a_astro, &ws.fwd.e2a_pos, st));
+    // Windows with more spikes than this use the pull gather instead of deposits.
+    // ASTROSIM_PUSH_LIMIT overrides it (the tests force the pull path with 0).
+    ws.push_limit = static_cast<u32>(std::max<u64>(1024, nN / 50));
+    if (const char* env = std::getenv("ASTROSIM_PUSH_LIMIT")) ws.push_limit = static_cast<u32>(std::strtoul(env, nullptr, 10));
+    const u32 cap = ws.push_limit + 1;
+    AS_TRY(ws.nin_cnt.alloc_zero(2 * nN, st));
+    AS_TRY(ws.ain_cnt.alloc_zero(2 * nA, st));
+    AS_TRY(ws.nin_ent.alloc(2 * nN * kInboxSlots * db));
+    AS_TRY(ws.ain_ent.alloc(2 * nA * kInboxSlots * db));
+    AS_TRY(ws.spk_word.alloc_zero(2 * nN, st));
+    AS_TRY(ws.spk_val.alloc_zero(2 * static_cast<u64>(ws.W) * nN * rb, st));
+    AS_TRY(ws.spk_list.alloc(2 * static_cast<u64>(cap)));
+    AS_TRY(ws.spk_count.alloc_zero(2, st));
+    AS_TRY(ws.sic_win.alloc_zero(2 * nA * ws.W * rb, st));
+    AS_TRY(ws.astro_active.alloc_zero(2 * ((nA + 31) / 32), st));
+    AS_TRY(ws.mode.alloc_zero(2, st));
+    AS_CUDA(cudaStreamSynchronize(st));
+    return Status::Ok();
+}
+
+namespace {
+template <typename R>
+Status launch_impl(const RunConsts& rc, StateBuffers& sb, Network& net, WindowState& ws, i64 raster_steps, i64 mark,
+                   i64 first, i64 count, cudaStream_t st, int block) {
+    StepPtrs<R> p = make_ptrs<R>(sb, net, rc, raster_steps);
+    WinPtrs<R> w = win_ptrs<R>(ws, rc);
+    const u32 astro_blocks = ceil_div(rc.n_astro, block);
+    const u32 neuron_blocks = ceil_div(rc.n_neurons, block);
+    const int W = ws.W;
+    const u32 push_blocks = std::max<u32>(1, std::min<u32>(148 * 8, ceil_div(ws.push_limit, 8)));
+    i64 t = first;
+    const i64 end = first + count;
+    while (t < end) {
+        const i64 k = t / W;
+        const int s0 = static_cast<int>(t - k * W);
+        const int s1 = static_cast<int>(std::min<i64>(W, end - k * W));
+        const int buf = static_cast<int>(k & 1);
+        window_kernel<R><<<astro_blocks + neuron_blocks, block, 0, st>>>(rc, p, w, k * W, s0, s1, buf, mark,
+                                                                          astro_blocks);
+        AS_CUDA(cudaGetLastError());
+        if (s1 == W) {
+            push_kernel<R><<<push_blocks, 256, 0, st>>>(w, rc.n_exc, net.sz.n_inh, rc.n_neurons, rc.n_astro, buf);
+            AS_CUDA(cudaGetLastError());
+        }
+        t = k * W + s1;
+    }
+    return Status::Ok();
+}
+}  // namespace
+
+Status window_launch(const RunConsts& rc, StateBuffers& sb, Network& net, bool fp32, WindowState& ws,
+                     i64 raster_steps, i64 mark_step, i64 first, i64 count, cudaStream_t st, int block) {
+    (void)block;
+    if (fp32) return launch_impl<float>(rc, sb, net, ws, raster_steps, mark_step, first, count, st, 128);
+    return launch_impl<double>(rc, sb, net, ws, raster_steps, mark_step, first, count, st, 128);
+}
+
+}  // namespace astrosim

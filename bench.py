@@ -1,0 +1,315 @@
+#!/usr/bin/env python3
+"""Benchmark of the tripartite network simulator on B200.
+
+Workload (the N=1e7 configuration): one network of N_total = 1e7 (8M excitatory,
+2M inhibitory AdEx neurons, 2M Li-Rinzel astrocytes, about 1.32e9 synapses),
+seed 1, dt = 0.1 ms, built on the device from (N, seed) exactly as the reference
+builds it.  One bench step = one network time step (dt).  `value` is net-steps/s
+of the FP32 form (FP64 accumulators) with the network resident in HBM; the plain
+FP64 path is measured beside it under "fp64".  `e2e` is the whole job through the
+C ABI: astrosim_create (device build) + the 100 ms pre-run and 500 ms recorded
+window (6000 steps) + astrosim_summary, timed on the host wall clock.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun with N > 1 every rank simulates its own replica network (seed 1 +
+rank); value = all ranks' net-steps / max-over-ranks device time.
+`--impl reference` runs the reference program itself (built from its own source
+for sm_100a into oracle/_ref) on the same configuration.
+"""
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "net-steps/s & syn-events/s at N=1e7 FP32 vs FP64; ensemble sims/s, p50/p99"
+N_TOTAL = 10_000_000
+SEED = 1
+DT = 0.1
+PRE_MS, SIM_MS = 100.0, 500.0
+
+
+def peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx = float(f[2])
+                except ValueError:
+                    continue
+                for name, val in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"),
+                                     f[5:9]):
+                    if val.lower() == "active":
+                        reasons.add(name)
+        finally:
+            try:
+                os.remove(self.path)
+            except OSError:
+                pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return ws, rank, local
+
+
+def dist_max(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def step_bytes(s, precision):
+    """Algorithmic bytes of one time step of the plain (per-step) path.
+
+    Per step every CSR source id is read once (4 B per edge visit, with the a2n rows
+    visited on every refresh step) and every cell's state is read and written once:
+    neurons 124 B (FP64) / 72 B (FP32), astrocytes 92 B / 48 B, plus one spike bit
+    per neuron.
+    """
+    e_visit = s["n_exc_edges"] + s["n_inh_edges"] + s["n_e2a_edges"] + s["n_sic_edges"]
+    nn = s["n_exc"] + s["n_inh"]
+    sn, sa = (124, 92) if precision == "fp64" else (72, 48)
+    return 4 * e_visit + nn * sn + s["n_astro"] * sa + nn / 8, e_visit
+
+
+def run_ours(args, ws, rank, local):
+    import astrosimgpu_cuda_b200 as asg
+
+    out = {}
+    seed = SEED + rank
+    # ---- e2e: config -> device build -> 6000 steps -> summary, through the C ABI
+    dist_barrier(ws)
+    t0 = time.perf_counter()
+    sim = asg.Simulation(n_total=N_TOTAL, seed=seed, pre_ms=PRE_MS, sim_ms=SIM_MS, precision="fp32", device=local)
+    total = sim.summary()["total_steps"]
+    sim.step(total)
+    summ = sim.summary()
+    counts = sim.spike_counts(0, total)
+    e2e_s = time.perf_counter() - t0
+    e2e_s = dist_max(e2e_s, ws)
+    out["e2e"] = {"value": ws * total / e2e_s, "unit": "net-steps/s", "seconds": e2e_s, "steps": total,
+                  "h2d_bytes_per_step": 120 / total,
+                  "d2h_bytes_per_step": (counts.nbytes + 8 * summ["n_astro"] + 200) / total,
+                  "includes": "astrosim_create (device connectivity + parameters) + astrosim_step x6000 + "
+                              "astrosim_summary + per-step spike counts"}
+    out["summary_fp32"] = {k: summ[k] for k in ("spikes_measured", "mean_rate_hz", "mean_ca", "active_astro",
+                                                "engaged_astro", "build_seconds", "n_exc_edges", "n_inh_edges",
+                                                "n_e2a_edges", "n_sic_edges")}
+
+    # ---- device-resident stepping, FP32 (the headline) then FP64
+    res = {}
+    for prec in ("fp32", "fp64"):
+        if prec == "fp64":
+            sim.close()
+            sim = asg.Simulation(n_total=N_TOTAL, seed=seed, pre_ms=PRE_MS, sim_ms=SIM_MS, precision="fp64",
+                                 device=local)
+            sim.step(total)  # same state point as the FP32 measurement
+        sim.step(args.warmup)
+        dist_barrier(ws)
+        with ClockSampler(local) as clk:
+            sim.step(args.steps)
+            ms = sim.last_step_ms()
+        ms = dist_max(ms, ws)
+        s = sim.summary()
+        b, e_visit = step_bytes(s, prec)
+        res[prec] = {"ms": ms, "clocks": clk.summary(), "bytes": b, "e_visit": e_visit, "summary": s}
+    sim.close()
+    return out, res
+
+
+def cpu_baseline(args):
+    """The FP64 oracle (OpenMP, every host core) stepping the same N=1e7 network."""
+    import numpy as np
+
+    import astrosimgpu_cuda_b200 as asg
+    from oracle import oracle
+
+    threads = os.cpu_count() or 1
+    with asg.Simulation(n_total=N_TOTAL, seed=SEED, pre_ms=PRE_MS, sim_ms=SIM_MS) as sim:
+        csrs = {k: sim.csr(k) for k in ("exc", "inh", "sic", "e2a")}
+    o = oracle.OracleSim(oracle_cfg(), threads=threads, csrs=csrs)
+    del csrs
+    o.step(1)
+    n = max(1, args.cpu_steps)
+    t = time.perf_counter()
+    o.step(n)
+    dt_s = time.perf_counter() - t
+    o.close()
+    return {"value": n / dt_s, "unit": "net-steps/s", "cores": threads, "kind": "port",
+            "sample": f"FP64 oracle, the N=1e7 seed-1 network (device-built CSR, identical to the reference's), "
+                      f"{n} time steps after 1 warm-up step, {dt_s:.1f} s",
+            "seconds": dt_s}
+
+
+def oracle_cfg():
+    from astrosimgpu_cuda_b200 import abi
+    return abi.default_config(n_total=N_TOTAL, seed=SEED, pre_ms=PRE_MS, sim_ms=SIM_MS)
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return None
+    binary = os.path.join(REPO, "oracle", "_ref", "astrosim_fused_ref_f32")
+    if not os.path.exists(binary):
+        return {"impl": "reference", "unavailable": "oracle/_ref/astrosim_fused_ref_f32 not built"}
+    steps = args.warmup + args.steps
+    cmd = [binary, "--n", str(N_TOTAL), "--seed", str(SEED), "--pre-ms", "0", "--sim-ms", f"{steps * DT:g}"]
+    t = time.perf_counter()
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=3600)
+    wall = time.perf_counter() - t
+    if r.returncode != 0:
+        return {"impl": "reference", "unavailable": f"reference exited {r.returncode}: {r.stderr.strip()[-200:]}"}
+    us = float(re.search(r"\(([0-9.]+) us/step", r.stdout).group(1))
+    build = float(re.search(r"built in ([0-9.]+) s", r.stdout).group(1))
+    value = 1e6 / us
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "net-steps/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": us / 1000.0, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "single network N_total=1e7 seed 1, dt 0.1 ms; the reference's -DASTROSIM_USE_FLOAT "
+                               "build (its FP32 network differs from the FP64 one)",
+                   "n_total": N_TOTAL, "seed": SEED, "steps_run": steps},
+        "cpu_baseline": {"value": value, "unit": "net-steps/s", "cores": 1, "kind": "reference",
+                         "sample": f"unmodified reference program built for sm_100a: serial host connectivity build "
+                                   f"({build:.1f} s) then {steps} steps on the B200; value from its printed us/step"},
+        "e2e": {"value": value, "unit": "net-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_host_build_s": build, "reference_process_wall_s": wall,
+        "reference_e2e_steps_per_s_incl_build": steps / wall,
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=100)
+    ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    ws, rank, local = dist_init()
+
+    if args.impl == "reference":
+        line = run_reference(args, ws, rank)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        return
+
+    extra, res = run_ours(args, ws, rank, local)
+    if rank != 0:
+        return
+    peak, peak_kind = peaks()
+    f32, f64 = res["fp32"], res["fp64"]
+    ms_step = f32["ms"] / args.steps
+    value = ws * args.steps / (f32["ms"] * 1e-3)
+    achieved = f32["bytes"] / (ms_step * 1e-3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "net-steps/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: the network is generated on the device from (N_total, seed) by the reference's "
+                "construction; no dataset",
+        "config": {"workload": "single network N_total=1e7 (8M exc, 2M inh AdEx, 2M Li-Rinzel astrocytes), seed 1, "
+                               "dt 0.1 ms; FP32 RK4 stages with FP64 V/w/Ca/IP3 accumulators; one step = one dt",
+                   "n_total": N_TOTAL, "seed": SEED, "dt_ms": DT,
+                   "timed_after": "the 6000-step e2e run plus the warm-up steps",
+                   "l2": "no flush: per-step working set (CSR 5.3 GB + state) is far larger than the 126 MB L2"},
+        "syn_events_per_s": f32["e_visit"] * value,
+        "fp64": {"value": ws * args.steps / (f64["ms"] * 1e-3), "unit": "net-steps/s",
+                 "ms_per_step": f64["ms"] / args.steps, "syn_events_per_s": f64["e_visit"] * ws * args.steps /
+                 (f64["ms"] * 1e-3), "clocks": f64["clocks"]},
+        "fp32_over_fp64": f64["ms"] / f32["ms"],
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_step": f32["bytes"]},
+        "e2e": extra["e2e"],
+        "gpu_launches": args.steps,
+        "clocks": f32["clocks"],
+        "summary_fp32": extra["summary_fp32"],
+    }
+    if not args.no_cpu_baseline and ws == 1:
+        try:
+            line["cpu_baseline"] = cpu_baseline(args)
+        except Exception as e:  # the baseline is reported, not required
+            line["cpu_baseline"] = {"value": None, "unavailable": str(e)[:200]}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

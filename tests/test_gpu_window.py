@@ -1,0 +1,53 @@
+"""The windowed engine (one launch per 1 ms window, spikes pushed into inboxes, or
+pulled from the previous window's spike words) gives bit-identical results to the
+per-step path, which itself matches the oracle and the reference (test_gpu_parity,
+test_gpu_reference_golden).  Both engines are forced through ASTROSIM_STEPPER and
+the pull fallback through ASTROSIM_PUSH_LIMIT."""
+import numpy as np
+import pytest
+
+import astrosimgpu_cuda_b200 as asg
+
+pytestmark = pytest.mark.gpu
+
+STATES = ("V", "w", "g_ex", "dg_ex", "g_in", "dg_in", "I_sic", "stp_x", "stp_u", "stp_t_last", "Ca", "IP3", "h",
+          "sic_factor")
+
+
+def run(monkeypatch, stepper, push_limit, chunks, **kw):
+    monkeypatch.setenv("ASTROSIM_STEPPER", stepper)
+    if push_limit is None:
+        monkeypatch.delenv("ASTROSIM_PUSH_LIMIT", raising=False)
+    else:
+        monkeypatch.setenv("ASTROSIM_PUSH_LIMIT", str(push_limit))
+    with asg.Simulation(**kw) as sim:
+        for c in chunks:
+            sim.step(c)
+        out = {k: sim.state(k) for k in STATES}
+        out["counts"] = sim.spike_counts()
+        out["summary"] = {k: v for k, v in sim.summary().items() if k not in ("build_seconds", "run_seconds")}
+        if kw.get("raster_steps"):
+            out["raster"] = sim.raster()
+    return out
+
+
+@pytest.mark.parametrize("n_total,seed,precision", [(500, 1, "fp64"), (5000, 2, "fp64"), (2000, 3, "fp32"),
+                                                    (20000, 7, "fp64"), (20000, 7, "fp32")])
+def test_windowed_push_and_pull_match_per_step_path(monkeypatch, n_total, seed, precision):
+    kw = dict(n_total=n_total, seed=seed, pre_ms=30, sim_ms=120, precision=precision, raster_steps=600)
+    chunks = (3, 17, 100, 1117, 263)
+    ref = run(monkeypatch, "plain", None, chunks, **kw)
+    for push_limit in (None, 0):
+        got = run(monkeypatch, "auto", push_limit, chunks, **kw)
+        for k in STATES + ("counts", "raster"):
+            np.testing.assert_array_equal(got[k], ref[k], err_msg=f"{k} push_limit={push_limit}")
+        assert got["summary"] == ref["summary"]
+    assert ref["counts"].sum() > 0
+
+
+def test_windowed_dt_quarter_ms(monkeypatch):
+    kw = dict(n_total=3000, seed=4, pre_ms=10, sim_ms=90, dt=0.25)  # D = 4 steps
+    ref = run(monkeypatch, "plain", None, (400,), **kw)
+    got = run(monkeypatch, "auto", None, (7, 393), **kw)
+    for k in STATES + ("counts",):
+        np.testing.assert_array_equal(got[k], ref[k], err_msg=k)
