@@ -338,8 +338,23 @@ Status build_sequential(const Sizes& sz, u64 seed, u64 c0, Network& net, cudaStr
     return make_error(ASTROSIM_ERR_CUDA, "skip tie-break table did not settle");
 }
 
+static double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+PhaseClock::PhaseClock(cudaStream_t s) : on(std::getenv("ASTROSIM_TIMING") != nullptr), st(s), t0(now_s()) {}
+
+void PhaseClock::mark(const char* what) {
+    if (!on) return;
+    cudaStreamSynchronize(st);
+    const double t = now_s();
+    std::fprintf(stderr, "[astrosim build] %-28s %8.3f ms\n", what, (t - t0) * 1e3);
+    t0 = t;
+}
+
 Status build_network(const Sizes& sz, u64 seed, const Biology& bio, const BuildOptions& opt, Network& net,
                      cudaStream_t st) {
+    PhaseClock pc(st);
     const auto t0 = std::chrono::steady_clock::now();
     net.sz = sz;
     net.seed = seed;
@@ -347,6 +362,7 @@ Status build_network(const Sizes& sz, u64 seed, const Biology& bio, const BuildO
     AS_TRY(scratch.alloc(1));
     u64 c0 = 0;
     AS_TRY(prologue_end(sz, seed, st, &c0, scratch.get()));
+    pc.mark("prologue");
     const double est = estimated_walk_draws(sz);
     // ASTROSIM_BUILDER=sequential|parallel forces one connectivity path (used by the
     // tests to run both paths on the same networks).
@@ -362,7 +378,9 @@ Status build_network(const Sizes& sz, u64 seed, const Biology& bio, const BuildO
         net.builder_path = 1;
         AS_TRY(build_parallel(sz, seed, c0, net, st));
     }
+    pc.mark("connectivity");
     AS_TRY(draw_cell_parameters(sz, seed, bio, net, st));
+    pc.mark("parameters");
     AS_CUDA(cudaStreamSynchronize(st));
     net.build_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     return Status::Ok();

@@ -63,6 +63,15 @@ __device__ __forceinline__ void pools_sequential(u64 seed, u32 n_neurons, u32 n_
     for (u32 post = 0; post < n_neurons; ++post) pool_one(seed, n_astro, c, pool + static_cast<u64>(post) * kPoolSize);
 }
 
+// Phase timing of the build, printed to stderr when ASTROSIM_TIMING is set.
+struct PhaseClock {
+    bool on;
+    cudaStream_t st;
+    double t0;
+    explicit PhaseClock(cudaStream_t s);
+    void mark(const char* what);
+};
+
 Status build_sequential(const Sizes& sz, u64 seed, u64 c0, Network& net, cudaStream_t st);
 Status build_parallel(const Sizes& sz, u64 seed, u64 c0, Network& net, cudaStream_t st);
 Status draw_cell_parameters(const Sizes& sz, u64 seed, const Biology& bio, Network& net, cudaStream_t st);

@@ -654,6 +654,7 @@ Status build_parallel(const Sizes& sz, u64 seed, u64 c0, Network& net, cudaStrea
         return build_sequential(sz, seed, c0, net, st);  // all-to-all networks are tiny
     const u32 nN = sz.n_neurons, nA = sz.n_astro;
     const u32 take = nA < kPoolSize ? nA : kPoolSize;
+    PhaseClock pc(st);
     DevBuf<int> err;
     AS_TRY(err.alloc_zero(1, st));
 
@@ -690,6 +691,7 @@ Status build_parallel(const Sizes& sz, u64 seed, u64 c0, Network& net, cudaStrea
     extra.release();
     prefix.release();
     prefix_new.release();
+    pc.mark("pools");
 
     // ---- 2. skip cache over every tape position the three sections can reach
     const double ne = sz.n_exc, ni = sz.n_inh, nn = nN, p = sz.p;
@@ -728,6 +730,7 @@ Status build_parallel(const Sizes& sz, u64 seed, u64 c0, Network& net, cudaStrea
         }
     }
 
+    pc.mark("skip cache");
     // ---- 3-4. every pre's start, section by section
     Sec s{};
     s.seed = seed;
@@ -746,6 +749,7 @@ Status build_parallel(const Sizes& sz, u64 seed, u64 c0, Network& net, cudaStrea
         u64 end = 0;
         AS_TRY(section_orbit(plans[k], s, start, err, orbits[k], &end, st));
         start = end;
+        pc.mark(plans[k].name);
     }
 
     // ---- 5. count, scan, emit
@@ -812,8 +816,10 @@ Status build_parallel(const Sizes& sz, u64 seed, u64 c0, Network& net, cudaStrea
     }
     cache.release();
     pool.release();
+    pc.mark("count + emit");
     const u64 counts[3] = {es.cap_exc, es.cap_inh, es.cap_third};
     AS_TRY(edge_lists_to_network(es.view(), counts, sz, net, st));
+    pc.mark("CSR sort");
 
     // The astrocyte out-degree cap (src/astrosim_fused.cu:702) drops a third-factor
     // edge only once an astrocyte already has 10000; with at most 10000 candidates

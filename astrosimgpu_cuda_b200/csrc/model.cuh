@@ -28,13 +28,29 @@ using u16 = std::uint16_t;
 // src/astrosim_fused.cu:127-135.  Every random quantity in the model is a
 // pure function of these three integers, which is what lets the device
 // generate any draw of the reference's sequential streams directly.
-__host__ __device__ __forceinline__ u64 rng_bits(u64 seed, u64 stream, u64 counter) {
-    u64 z = seed;
-    z += stream * 0x9E3779B97F4A7C15ULL;
-    z += counter * 0xBF58476D1CE4E5B9ULL;
+constexpr u64 kStreamMul = 0x9E3779B97F4A7C15ULL;
+constexpr u64 kCounterMul = 0xBF58476D1CE4E5B9ULL;
+
+// The mixing half of the hash, applied to seed + stream * kStreamMul + counter * kCounterMul.
+__host__ __device__ __forceinline__ u64 rng_mix(u64 z) {
     z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
     z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
     return z ^ (z >> 31);
+}
+
+__host__ __device__ __forceinline__ u64 rng_bits(u64 seed, u64 stream, u64 counter) {
+    u64 z = seed;
+    z += stream * kStreamMul;
+    z += counter * kCounterMul;
+    return rng_mix(z);
+}
+
+// Stream base seed + stream * kStreamMul: the draws of one (seed, stream) are
+// rng_mix(base + counter * kCounterMul).  Per-step streams step * S + cell advance
+// the base by S * kStreamMul each step, so a loop over steps needs one 64-bit add.
+__host__ __device__ __forceinline__ u64 rng_base(u64 seed, u64 stream) { return seed + stream * kStreamMul; }
+__host__ __device__ __forceinline__ double rng_uniform_at(u64 base, u64 counter) {
+    return static_cast<double>(rng_mix(base + counter * kCounterMul) >> 11) * (1.0 / 9007199254740992.0);
 }
 
 // 53-bit uniform in [0, 1): src/astrosim_fused.cu:137-141 (double build).
@@ -81,6 +97,31 @@ __host__ __device__ __forceinline__ int rng_poisson_knuth(u64 seed, u64 stream, 
     return count;
 }
 
+// rng_poisson_knuth on a precomputed stream base.  `lim53` = floor(exp(-lambda) * 2^53):
+// the first draw u0 = m * 2^-53 exceeds the limit exactly when m > lim53, so the
+// common zero-event case needs no floating point at all.
+__host__ __device__ __forceinline__ int rng_poisson_at(u64 base, double lambda, double limit, u64 lim53) {
+    if (lambda <= 0.0) return 0;
+    if (lambda > 30.0) {
+        double u1 = rng_uniform_at(base, 0);
+        if (u1 <= 1e-300) u1 = 1e-300;
+        const double u2 = rng_uniform_at(base, 1);
+        const double z = sqrt(-2.0 * log(u1)) * cos(kTwoPi * u2);
+        const double v = lambda + sqrt(lambda) * z;
+        return v < 0.0 ? 0 : static_cast<int>(v + 0.5);
+    }
+    const u64 m = rng_mix(base) >> 11;
+    if (m <= lim53) return 0;
+    double product = static_cast<double>(m) * (1.0 / 9007199254740992.0);
+    int count = 0;
+    u64 c = 1;
+    do {
+        ++count;
+        product *= rng_uniform_at(base, c++);
+    } while (product > limit);
+    return count;
+}
+
 // Stream-selection constants of the per-step draws (src/astrosim_fused.cu:395, 404, 476, 499).
 constexpr u64 kAstroPoissonKey = 0xC2B2AE3D27D4EB4FULL;
 constexpr u64 kAstroNoiseKey = 0x9E3779B97F4A7C15ULL;
@@ -120,6 +161,8 @@ struct AstroK {
     double Kd_IP3_1, Kd_IP3_2, Kd_act, Kd_inh, Km_SERCA;
     double k_IP3R, rate_IP3R, rate_L, rate_SERCA, ratio_ER_cyt;
     double SIC_scale, SIC_th;
+    // Folded constants of the FP32 form (its stages multiply by reciprocals).
+    float f_inv_ratio, f_ratio_rate_IP3R, f_ratio_rate_L, f_k_Kd_inh, f_Km2;
 };
 
 // AdEx neuron constants for one population (src/astrosim_fused.cu:228-232).
@@ -127,6 +170,11 @@ struct NeuronK {
     double C_m, g_L, E_L, V_th, Delta_T, a, tau_w;
     double V_peak, t_ref, E_ex, E_in, tau_syn_ex, tau_syn_in, I_e;
     double psc_init_ex, psc_init_in;
+    // 1 / Delta_T when Delta_T is a power of two (then x / Delta_T == x * (1 / Delta_T)
+    // exactly in IEEE arithmetic), else 0.
+    double inv_Delta_T_pow2;
+    // Folded constants of the FP32 form.
+    float f_gL_DT, f_inv_DT, f_inv_Cm, f_inv_tauw;
 };
 
 // Biology defaults, compiled into the reference (src/astrosim_fused.cu:742-781).
@@ -169,6 +217,11 @@ inline AstroK astro_constants(const Biology& b) {  // src/astrosim_fused.cu:935-
     k.Kd_IP3_1 = b.Kd_IP3_1; k.Kd_IP3_2 = b.Kd_IP3_2; k.Kd_act = b.Kd_act; k.Kd_inh = b.Kd_inh;
     k.Km_SERCA = b.Km_SERCA; k.k_IP3R = b.k_IP3R; k.rate_IP3R = b.rate_IP3R; k.rate_L = b.rate_L;
     k.rate_SERCA = b.rate_SERCA; k.ratio_ER_cyt = b.ratio_ER_cyt; k.SIC_scale = b.SIC_scale; k.SIC_th = b.SIC_th;
+    k.f_inv_ratio = static_cast<float>(1.0 / b.ratio_ER_cyt);
+    k.f_ratio_rate_IP3R = static_cast<float>(b.ratio_ER_cyt * b.rate_IP3R);
+    k.f_ratio_rate_L = static_cast<float>(b.ratio_ER_cyt * b.rate_L);
+    k.f_k_Kd_inh = static_cast<float>(b.k_IP3R * b.Kd_inh);
+    k.f_Km2 = static_cast<float>(b.Km_SERCA * b.Km_SERCA);
     return k;
 }
 
@@ -190,6 +243,13 @@ inline NeuronK neuron_constants(const Biology& b, bool exc) {  // src/astrosim_f
     k.I_e = 0.0;
     k.psc_init_ex = 2.7182818284590452353602874713527 / k.tau_syn_ex;
     k.psc_init_in = 2.7182818284590452353602874713527 / k.tau_syn_in;
+    int ex = 0;
+    const double mant = std::frexp(k.Delta_T, &ex);
+    k.inv_Delta_T_pow2 = (k.Delta_T > 0.0 && mant == 0.5) ? 1.0 / k.Delta_T : 0.0;
+    k.f_gL_DT = static_cast<float>(k.g_L * k.Delta_T);
+    k.f_inv_DT = static_cast<float>(1.0 / k.Delta_T);
+    k.f_inv_Cm = static_cast<float>(1.0 / k.C_m);
+    k.f_inv_tauw = static_cast<float>(1.0 / k.tau_w);
     return k;
 }
 
@@ -226,18 +286,59 @@ __device__ __forceinline__ double exp_r(double x) { return exp(x); }
 __device__ __forceinline__ float exp_r(float x) { return expf(x); }
 
 // AdEx: src/astrosim_fused.cu:281-290 (operand order kept).
-template <typename R>
-__device__ __forceinline__ void neuron_rhs(const NeuronK& p, R V, R w, R g_ex, R g_in, R I_ext, R& dV, R& dw) {
-    const R V_peak = static_cast<R>(p.V_peak);
-    const R Vc = V < V_peak ? V : V_peak;
-    const R I_spike = static_cast<R>(p.g_L) * static_cast<R>(p.Delta_T) *
-                      exp_r((Vc - static_cast<R>(p.V_th)) / static_cast<R>(p.Delta_T));
-    const R I_syn_ex = g_ex * (Vc - static_cast<R>(p.E_ex));
-    const R I_syn_in = g_in * (Vc - static_cast<R>(p.E_in));
-    dV = (-static_cast<R>(p.g_L) * (Vc - static_cast<R>(p.E_L)) + I_spike - I_syn_ex - I_syn_in - w +
-          static_cast<R>(p.I_e) + I_ext) /
-         static_cast<R>(p.C_m);
-    dw = (static_cast<R>(p.a) * (Vc - static_cast<R>(p.E_L)) - w) / static_cast<R>(p.tau_w);
+__device__ __forceinline__ void neuron_rhs(const NeuronK& p, double V, double w, double g_ex, double g_in,
+                                           double I_ext, double& dV, double& dw) {
+    const double Vc = V < p.V_peak ? V : p.V_peak;
+    const double arg = p.inv_Delta_T_pow2 != 0.0 ? (Vc - p.V_th) * p.inv_Delta_T_pow2 : (Vc - p.V_th) / p.Delta_T;
+    const double I_spike = p.g_L * p.Delta_T * exp(arg);
+    const double I_syn_ex = g_ex * (Vc - p.E_ex);
+    const double I_syn_in = g_in * (Vc - p.E_in);
+    dV = (-p.g_L * (Vc - p.E_L) + I_spike - I_syn_ex - I_syn_in - w + p.I_e + I_ext) / p.C_m;
+    dw = (p.a * (Vc - p.E_L) - w) / p.tau_w;
+}
+
+// The FP32 form of the same right-hand side: reciprocal multiplies and the
+// hardware exponential (stage arithmetic only; V and w accumulate in double).
+__device__ __forceinline__ void neuron_rhs(const NeuronK& p, float V, float w, float g_ex, float g_in, float I_ext,
+                                           float& dV, float& dw) {
+    const float V_peak = static_cast<float>(p.V_peak), E_L = static_cast<float>(p.E_L);
+    const float Vc = V < V_peak ? V : V_peak;
+    const float I_spike = p.f_gL_DT * __expf((Vc - static_cast<float>(p.V_th)) * p.f_inv_DT);
+    const float I_syn_ex = g_ex * (Vc - static_cast<float>(p.E_ex));
+    const float I_syn_in = g_in * (Vc - static_cast<float>(p.E_in));
+    dV = (-static_cast<float>(p.g_L) * (Vc - E_L) + I_spike - I_syn_ex - I_syn_in - w + static_cast<float>(p.I_e) +
+          I_ext) * p.f_inv_Cm;
+    dw = (static_cast<float>(p.a) * (Vc - E_L) - w) * p.f_inv_tauw;
+}
+
+// The FP32 form of the Li-Rinzel right-hand side (see astro_rhs).
+__device__ __forceinline__ void astro_rhs_fast(const AstroK& c, float Ca_tot, float IP3_0, float inv_tau_IP3,
+                                               float Ca, float IP3, float h, float noise, float& dCa, float& dIP3,
+                                               float& dh) {
+    const float Ca_ER = (Ca_tot - Ca) * c.f_inv_ratio;
+    const float m_inf = __fdividef(IP3, IP3 + static_cast<float>(c.Kd_IP3_1));
+    const float n_inf = __fdividef(Ca, Ca + static_cast<float>(c.Kd_act));
+    const float m3 = m_inf * m_inf * m_inf;
+    const float n3 = n_inf * n_inf * n_inf;
+    const float h3 = h * h * h;
+    const float J_channel = c.f_ratio_rate_IP3R * m3 * n3 * h3 * (Ca_ER - Ca);
+    const float J_pump = __fdividef(static_cast<float>(c.rate_SERCA) * Ca * Ca, c.f_Km2 + Ca * Ca);
+    const float J_leak = c.f_ratio_rate_L * (Ca_ER - Ca);
+    const float alpha_h = __fdividef(c.f_k_Kd_inh * (IP3 + static_cast<float>(c.Kd_IP3_1)),
+                                     IP3 + static_cast<float>(c.Kd_IP3_2));
+    const float beta_h = static_cast<float>(c.k_IP3R) * Ca;
+    dCa = J_channel - J_pump + J_leak + noise;
+    dIP3 = (IP3_0 - IP3) * inv_tau_IP3;
+    dh = alpha_h * (1.0f - h) - beta_h * h;
+}
+
+// Box-Muller in float from one stream (counters 0 and 1): the noise draws of the FP32 form.
+__device__ __forceinline__ float normal_fast(u64 base) {
+    const u32 a = static_cast<u32>(rng_mix(base) >> 40);
+    const u32 b = static_cast<u32>(rng_mix(base + kCounterMul) >> 40);
+    const float u1 = (static_cast<float>(a) + 0.5f) * (1.0f / 16777216.0f);
+    const float u2 = static_cast<float>(b) * (1.0f / 16777216.0f);
+    return sqrtf(-2.0f * __logf(u1)) * __cosf(static_cast<float>(kTwoPi) * u2);
 }
 
 }  // namespace astrosim

@@ -12,6 +12,7 @@
 #include "sim.cuh"
 #include "step_kernels.cuh"
 #include "window.cuh"
+#include "builder_internal.cuh"
 
 namespace astrosim {
 
@@ -180,6 +181,9 @@ Status Simulation::create(const astrosim_config& cfg) {
         rc.limit_astro = h[0];
         rc.limit_exc = h[1];
         rc.limit_inh = h[2];
+        rc.lim53_astro = static_cast<u64>(std::floor(h[0] * 9007199254740992.0));
+        rc.lim53_exc = static_cast<u64>(std::floor(h[1] * 9007199254740992.0));
+        rc.lim53_inh = static_cast<u64>(std::floor(h[2] * 9007199254740992.0));
     }
 
     pre_steps_ = static_cast<i64>(cfg.pre_ms / cfg.dt + 0.5);
@@ -210,7 +214,9 @@ Status Simulation::create(const astrosim_config& cfg) {
         AS_TRY(st_.sic_ring_raw.alloc_zero(static_cast<u64>(rc.slots) * nA * rbytes, stream_));
     } else {
         win_ = new WindowState();
+        PhaseClock pc(stream_);
         AS_TRY(window_setup(rc, net_, fp32_, *win_, stream_));
+        pc.mark("window set-up (forward CSRs)");
     }
     AS_TRY(st_.sic_last_raw.alloc(nA * rbytes));
     AS_TRY(st_.raster.alloc_zero(static_cast<u64>(cfg.raster_steps) * rc.words, stream_));

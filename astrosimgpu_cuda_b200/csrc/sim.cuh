@@ -24,6 +24,7 @@ struct RunConsts {
     double lambda_astro, limit_astro, weight_astro, noise_astro;
     double lambda_exc, limit_exc, weight_exc, noise_exc;
     double lambda_inh, limit_inh, weight_inh, noise_inh;
+    u64 lim53_astro, lim53_exc, lim53_inh;  // floor(exp(-lambda) * 2^53) for the integer first test
     bool independent_noise;
     bool stp_enabled;
     double stp_U, stp_tau_rec, stp_tau_fac;

@@ -3,6 +3,8 @@
 // V, w, Ca and IP3 always accumulate in double.
 #pragma once
 
+#include <type_traits>
+
 #include "model.cuh"
 #include "sim.cuh"
 
@@ -43,21 +45,33 @@ __device__ __forceinline__ R gather_spikes(const u32* __restrict__ rs, const u32
 
 // Li-Rinzel RK4 with clamps (src/astrosim_fused.cu:255-278); noise held over the stages.
 template <typename R>
+__device__ __forceinline__ void astro_stage(const AstroK& c, R Ct, R I0, R tI, R inv_tI, R Ca, R IP3, R h, R noise,
+                                            R& dCa, R& dIP3, R& dh) {
+    if constexpr (std::is_same<R, float>::value) {
+        astro_rhs_fast(c, Ct, I0, inv_tI, Ca, IP3, h, noise, dCa, dIP3, dh);
+    } else {
+        (void)inv_tI;
+        astro_rhs<R>(c, Ct, I0, tI, Ca, IP3, h, noise, dCa, dIP3, dh);
+    }
+}
+
+template <typename R>
 __device__ __forceinline__ void astro_advance(const AstroK& c, double Ca_tot, double IP3_0, double tau_IP3,
                                               double delta_IP3, R ip3_input, R noise, double h_step, int substeps,
                                               double& Ca, double& IP3, R& h) {
     if (ip3_input != static_cast<R>(0.0)) IP3 += delta_IP3 * static_cast<double>(ip3_input);
     const R hs = static_cast<R>(h_step);
     const R Ct = static_cast<R>(Ca_tot), I0 = static_cast<R>(IP3_0), tI = static_cast<R>(tau_IP3);
+    const R inv_tI = static_cast<R>(1.0) / tI;  // used by the FP32 form only
     for (int s = 0; s < substeps; ++s) {
         const R ca = static_cast<R>(Ca), ip = static_cast<R>(IP3);
         R k1c, k1i, k1h, k2c, k2i, k2h, k3c, k3i, k3h, k4c, k4i, k4h;
-        astro_rhs<R>(c, Ct, I0, tI, ca, ip, h, noise, k1c, k1i, k1h);
-        astro_rhs<R>(c, Ct, I0, tI, ca + static_cast<R>(0.5) * hs * k1c, ip + static_cast<R>(0.5) * hs * k1i,
-                     h + static_cast<R>(0.5) * hs * k1h, noise, k2c, k2i, k2h);
-        astro_rhs<R>(c, Ct, I0, tI, ca + static_cast<R>(0.5) * hs * k2c, ip + static_cast<R>(0.5) * hs * k2i,
-                     h + static_cast<R>(0.5) * hs * k2h, noise, k3c, k3i, k3h);
-        astro_rhs<R>(c, Ct, I0, tI, ca + hs * k3c, ip + hs * k3i, h + hs * k3h, noise, k4c, k4i, k4h);
+        astro_stage<R>(c, Ct, I0, tI, inv_tI, ca, ip, h, noise, k1c, k1i, k1h);
+        astro_stage<R>(c, Ct, I0, tI, inv_tI, ca + static_cast<R>(0.5) * hs * k1c, ip + static_cast<R>(0.5) * hs * k1i,
+                       h + static_cast<R>(0.5) * hs * k1h, noise, k2c, k2i, k2h);
+        astro_stage<R>(c, Ct, I0, tI, inv_tI, ca + static_cast<R>(0.5) * hs * k2c, ip + static_cast<R>(0.5) * hs * k2i,
+                       h + static_cast<R>(0.5) * hs * k2h, noise, k3c, k3i, k3h);
+        astro_stage<R>(c, Ct, I0, tI, inv_tI, ca + hs * k3c, ip + hs * k3i, h + hs * k3h, noise, k4c, k4i, k4h);
         Ca += static_cast<double>((hs / static_cast<R>(6.0)) *
                                   (k1c + static_cast<R>(2.0) * k2c + static_cast<R>(2.0) * k3c + k4c));
         IP3 += static_cast<double>((hs / static_cast<R>(6.0)) *
@@ -83,21 +97,26 @@ struct AstroRegs {
 // Everything astrocyte `a` does in step `step` once its delayed spike sum is known
 // (src/astrosim_fused.cu:390-417): Poisson IP3 drive, noise, RK4, SIC factor.
 template <typename R>
-__device__ __forceinline__ R astro_advance_step(const RunConsts& rc, AstroRegs<R>& s, R gathered, u32 a, i64 step) {
+__device__ __forceinline__ R astro_advance_step(const RunConsts& rc, AstroRegs<R>& s, R gathered, u32 a, i64 step,
+                                                u64 poisson_base, u64 noise_base) {
     R ip3_input = static_cast<R>(rc.w_n2a) * gathered;
     if (rc.lambda_astro > 0.0) {
-        const int ev = rng_poisson_knuth(rc.seed ^ kAstroPoissonKey, static_cast<u64>(step) * kCellStride + a,
-                                         rc.lambda_astro, rc.limit_astro);
+        const int ev = rng_poisson_at(poisson_base, rc.lambda_astro, rc.limit_astro, rc.lim53_astro);
         if (ev > 0) ip3_input += static_cast<R>(rc.weight_astro) * static_cast<R>(ev);
     }
     R noise = static_cast<R>(0.0);
     if (rc.noise_astro > 0.0) {
-        if (rc.independent_noise)
-            noise = static_cast<R>(rc.noise_astro *
-                                   rng_normal(rc.seed ^ kAstroNoiseKey, static_cast<u64>(step) * kCellStride + a));
-        else
-            noise = static_cast<R>(rc.noise_astro * rng_normal(rc.seed ^ kAstroNoiseKey,
-                                                               static_cast<u64>(step / rc.steps_per_noise)));
+        u64 base = noise_base;
+        if (!rc.independent_noise)
+            base = rng_base(rc.seed ^ kAstroNoiseKey, static_cast<u64>(step / rc.steps_per_noise));
+        if constexpr (std::is_same<R, float>::value) {
+            noise = static_cast<float>(rc.noise_astro) * normal_fast(base);
+        } else {
+            double u1 = rng_uniform_at(base, 0);  // rng_normal (src/astrosim_fused.cu:143-149)
+            if (u1 <= 1e-300) u1 = 1e-300;
+            const double u2 = rng_uniform_at(base, 1);
+            noise = rc.noise_astro * (sqrt(-2.0 * log(u1)) * cos(kTwoPi * u2));
+        }
     }
     astro_advance<R>(rc.ak, s.Ca_tot, s.IP3_0, s.tau_IP3, s.delta_IP3, ip3_input, noise, rc.h_step, rc.substeps,
                      s.Ca, s.IP3, s.h);
@@ -108,6 +127,13 @@ __device__ __forceinline__ R astro_advance_step(const RunConsts& rc, AstroRegs<R
     return factor;
 }
 
+// Stream bases of a cell's per-step draws (stream = step * 1000003 + cell); the next
+// step's base is this one plus kStepAdvance.
+constexpr u64 kStepAdvance = kCellStride * kStreamMul;
+__device__ __forceinline__ u64 step_base(u64 seed, u64 key, i64 step, u32 cell) {
+    return rng_base(seed ^ key, static_cast<u64>(step) * kCellStride + cell);
+}
+
 // One astrocyte for step `step` on the per-step rings (src/astrosim_fused.cu:374-427).
 template <typename R>
 __device__ __forceinline__ void astro_cell_step(const RunConsts& rc, const StepPtrs<R>& p, u32 a, i64 step) {
@@ -116,7 +142,8 @@ __device__ __forceinline__ void astro_cell_step(const RunConsts& rc, const StepP
     const R gathered = gather_spikes<R>(p.e2a_rs, p.e2a_src, a, p.bits + static_cast<u64>(read_slot) * rc.words,
                                         p.val + static_cast<u64>(read_slot) * rc.n_neurons);
     AstroRegs<R> s{p.Ca[a], p.IP3[a], p.h[a], p.Ca_tot[a], p.IP3_0[a], p.tau_IP3[a], p.delta_IP3[a]};
-    const R factor = astro_advance_step<R>(rc, s, gathered, a, step);
+    const R factor = astro_advance_step<R>(rc, s, gathered, a, step, step_base(rc.seed, kAstroPoissonKey, step, a),
+                                           step_base(rc.seed, kAstroNoiseKey, step, a));
     p.Ca[a] = s.Ca;
     p.IP3[a] = s.IP3;
     p.h[a] = s.h;
@@ -140,14 +167,14 @@ struct NeuronRegs {
 template <typename R>
 __device__ __forceinline__ bool neuron_advance_step(const RunConsts& rc, const NeuronK& pk, bool excitatory,
                                                     NeuronRegs<R>& n, R exc_sum, R inh_sum, bool sic_refresh,
-                                                    R sic_sum, bool has_noise, double noise, u32 j, i64 step,
+                                                    R sic_sum, bool has_noise, double noise, u64 poisson_base,
                                                     R ex_decay, R in_decay) {
     R exc_input = static_cast<R>(rc.w_e) * exc_sum;
     const R inh_input = static_cast<R>(-rc.w_i) * inh_sum;
     const double lambda = excitatory ? rc.lambda_exc : rc.lambda_inh;
     if (lambda > 0.0) {
-        const int ev = rng_poisson_knuth(rc.seed ^ kNeuronPoissonKey, static_cast<u64>(step) * kCellStride + j, lambda,
-                                         excitatory ? rc.limit_exc : rc.limit_inh);
+        const int ev = rng_poisson_at(poisson_base, lambda, excitatory ? rc.limit_exc : rc.limit_inh,
+                                      excitatory ? rc.lim53_exc : rc.lim53_inh);
         if (ev > 0) exc_input += static_cast<R>(excitatory ? rc.weight_exc : rc.weight_inh) * static_cast<R>(ev);
     }
     if (sic_refresh) n.I_sic = static_cast<R>(rc.w_a2n) * sic_sum;
@@ -168,19 +195,19 @@ __device__ __forceinline__ bool neuron_advance_step(const RunConsts& rc, const N
         if (refractory > 0) {
             V = n.V_reset;
             R dV, dw;
-            neuron_rhs<R>(pk, static_cast<R>(V), static_cast<R>(w), g_ex, g_in, I_ext, dV, dw);
+            neuron_rhs(pk, static_cast<R>(V), static_cast<R>(w), g_ex, g_in, I_ext, dV, dw);
             w += static_cast<double>(hs * dw);
         } else {
             const R g_ex_mid = static_cast<R>(0.5) * (g_ex + g_ex_next);
             const R g_in_mid = static_cast<R>(0.5) * (g_in + g_in_next);
             const R v = static_cast<R>(V), ww = static_cast<R>(w);
             R k1V, k1w, k2V, k2w, k3V, k3w, k4V, k4w;
-            neuron_rhs<R>(pk, v, ww, g_ex, g_in, I_ext, k1V, k1w);
-            neuron_rhs<R>(pk, v + static_cast<R>(0.5) * hs * k1V, ww + static_cast<R>(0.5) * hs * k1w, g_ex_mid,
+            neuron_rhs(pk, v, ww, g_ex, g_in, I_ext, k1V, k1w);
+            neuron_rhs(pk, v + static_cast<R>(0.5) * hs * k1V, ww + static_cast<R>(0.5) * hs * k1w, g_ex_mid,
                           g_in_mid, I_ext, k2V, k2w);
-            neuron_rhs<R>(pk, v + static_cast<R>(0.5) * hs * k2V, ww + static_cast<R>(0.5) * hs * k2w, g_ex_mid,
+            neuron_rhs(pk, v + static_cast<R>(0.5) * hs * k2V, ww + static_cast<R>(0.5) * hs * k2w, g_ex_mid,
                           g_in_mid, I_ext, k3V, k3w);
-            neuron_rhs<R>(pk, v + hs * k3V, ww + hs * k3w, g_ex_next, g_in_next, I_ext, k4V, k4w);
+            neuron_rhs(pk, v + hs * k3V, ww + hs * k3w, g_ex_next, g_in_next, I_ext, k4V, k4w);
             V += static_cast<double>((hs / static_cast<R>(6.0)) *
                                      (k1V + static_cast<R>(2.0) * k2V + static_cast<R>(2.0) * k3V + k4V));
             w += static_cast<double>((hs / static_cast<R>(6.0)) *
@@ -227,6 +254,20 @@ __device__ __forceinline__ R stp_on_spike(const RunConsts& rc, R& sx, R& su, dou
     return static_cast<R>(x * u);
 }
 
+// noise_std * N(0,1) of neuron j for noise index idx (src/astrosim_fused.cu:494-504).
+template <typename R>
+__device__ __forceinline__ double neuron_noise(const RunConsts& rc, double nstd, u64 idx, u32 j) {
+    const u64 base = rng_base(rc.seed ^ kNeuronNoiseKey, idx * kNoiseStride + j);
+    if constexpr (std::is_same<R, float>::value) {
+        return static_cast<double>(static_cast<float>(nstd) * normal_fast(base));
+    } else {
+        double u1 = rng_uniform_at(base, 0);
+        if (u1 <= 1e-300) u1 = 1e-300;
+        const double u2 = rng_uniform_at(base, 1);
+        return nstd * (sqrt(-2.0 * log(u1)) * cos(kTwoPi * u2));
+    }
+}
+
 // One neuron for step `step` on the per-step rings (src/astrosim_fused.cu:433-587).
 // Returns whether it spiked and the value its ring entry carries.
 template <typename R>
@@ -251,14 +292,15 @@ __device__ __forceinline__ bool neuron_cell_step(const RunConsts& rc, const Step
     }
     const double nstd = excitatory ? rc.noise_exc : rc.noise_inh;
     const bool has_noise = nstd > 0.0 && rc.independent_noise;
-    const double noise = has_noise ? nstd * rng_normal(rc.seed ^ kNeuronNoiseKey, noise_idx * kNoiseStride + j) : 0.0;
+    const double noise = has_noise ? neuron_noise<R>(rc, nstd, noise_idx, j) : 0.0;
     NeuronRegs<R> n{p.V[j], p.w[j], p.V_reset[j], p.b[j], p.g_ex[j], p.dg_ex[j], p.g_in[j], p.dg_in[j], p.I_sic[j],
                     p.refr[j]};
     const R hs = static_cast<R>(rc.h_step);
     const R ex_decay = exp_r(-hs / static_cast<R>(pk.tau_syn_ex));
     const R in_decay = exp_r(-hs / static_cast<R>(pk.tau_syn_in));
     const bool spiked = neuron_advance_step<R>(rc, pk, excitatory, n, exc_sum, inh_sum, sic_refresh, sic_sum,
-                                               has_noise, noise, j, step, ex_decay, in_decay);
+                                               has_noise, noise, step_base(rc.seed, kNeuronPoissonKey, step, j),
+                                               ex_decay, in_decay);
     p.V[j] = n.V;
     p.w[j] = n.w;
     p.g_ex[j] = n.g_ex;

@@ -130,9 +130,13 @@ __global__ void __launch_bounds__(128) window_kernel(RunConsts rc, StepPtrs<R> p
             unsigned char ever = p.ever_active[a];
             R* out = w.sic_win + (static_cast<u64>(buf) * rc.n_astro + a) * W;
             R factor = static_cast<R>(0.0);
+            u64 pbase = step_base(rc.seed, kAstroPoissonKey, win_start + s_begin, a);
+            u64 nbase = step_base(rc.seed, kAstroNoiseKey, win_start + s_begin, a);
             for (int st = s_begin; st < s_end; ++st) {
                 const i64 t = win_start + st;
-                factor = astro_advance_step<R>(rc, s, ip3_input ? acc[st] : static_cast<R>(0.0), a, t);
+                factor = astro_advance_step<R>(rc, s, ip3_input ? acc[st] : static_cast<R>(0.0), a, t, pbase, nbase);
+                pbase += kStepAdvance;
+                nbase += kStepAdvance;
                 out[st] = factor;
                 if (factor > static_cast<R>(0.0)) {
                     ever = 1;
@@ -212,6 +216,7 @@ __global__ void __launch_bounds__(128) window_kernel(RunConsts rc, StepPtrs<R> p
     const bool has_noise = nstd > 0.0 && rc.independent_noise;
     u64 noise_idx_cached = ~0ull;
     double noise = 0.0;
+    u64 pbase = step_base(rc.seed, kNeuronPoissonKey, win_start + s_begin, j);
     u32 word = 0;
     R* vout = w.spk_val + static_cast<u64>(buf) * W * nN;
     for (int st = s_begin; st < s_end; ++st) {
@@ -220,14 +225,15 @@ __global__ void __launch_bounds__(128) window_kernel(RunConsts rc, StepPtrs<R> p
         if (has_noise) {
             const u64 idx = static_cast<u64>(t / rc.steps_per_noise);
             if (idx != noise_idx_cached) {
-                noise = nstd * rng_normal(rc.seed ^ kNeuronNoiseKey, idx * kNoiseStride + j);
+                noise = neuron_noise<R>(rc, nstd, idx, j);
                 noise_idx_cached = idx;
             }
         }
         const R zero = static_cast<R>(0.0);
         const bool spiked = neuron_advance_step<R>(
             rc, pk, excitatory, n, syn_input ? ex_acc[st] : zero, syn_input ? in_acc[st] : zero, refresh,
-            sic_input ? sic_acc[st] : zero, has_noise, noise, j, t, ex_decay, in_decay);
+            sic_input ? sic_acc[st] : zero, has_noise, noise, pbase, ex_decay, in_decay);
+        pbase += kStepAdvance;
         if (spiked) {
             const R out = stp_on_spike<R>(rc, p.stp_x[j], p.stp_u[j], p.stp_t[j], t);
             vout[static_cast<u64>(st) * nN + j] = out;
