@@ -13,6 +13,7 @@
 #include "step_kernels.cuh"
 #include "window.cuh"
 #include "builder_internal.cuh"
+#include "reduce.cuh"
 
 namespace astrosim {
 
@@ -221,6 +222,7 @@ Status Simulation::create(const astrosim_config& cfg) {
     AS_TRY(st_.sic_last_raw.alloc(nA * rbytes));
     AS_TRY(st_.raster.alloc_zero(static_cast<u64>(cfg.raster_steps) * rc.words, stream_));
     AS_TRY(ensure_counts(std::max<i64>(total_steps_, 1)));
+    AS_TRY(st_.reduce_raw.alloc(reduce_blocks(sz.n_astro) * sizeof(AstroPartial) + sizeof(AstroTotals)));
     const unsigned grid = ceil_div(std::max<u64>(nN, nA), 256);
     if (fp32_) {
         auto p = make_ptrs<float>(st_, net_, rc, cfg.raster_steps);
@@ -353,23 +355,17 @@ Status Simulation::summary(astrosim_summary_t& out) {
     out.spikes_measured = tot - before;
     out.mean_rate_hz = static_cast<double>(out.spikes_measured) /
                        (static_cast<double>(sz.n_neurons) * (cfg_.sim_ms * 1e-3));
-    std::vector<double> ca(sz.n_astro);
-    AS_TRY(get_state(ASTROSIM_STATE_CA, ca.data(), ca.size()));
-    double mean = 0.0;
-    u32 active = 0;
-    for (double v : ca) {  // src/astrosim_fused.cu:1113-1119, in astrocyte order
-        mean += v;
-        if ((v - bio_.SIC_th) * 1000.0 > 1.0) ++active;
-    }
-    mean /= std::max<u32>(1, sz.n_astro);
-    std::vector<unsigned char> ea(sz.n_astro);
-    AS_CUDA(cudaMemcpyAsync(ea.data(), st_.ever_active.get(), sz.n_astro, cudaMemcpyDeviceToHost, stream_));
+    // mean calcium, final-step threshold count and engaged count (src/astrosim_fused.cu:1111-1125),
+    // reduced on the device
+    AstroPartial* parts = reinterpret_cast<AstroPartial*>(st_.reduce_raw.get());
+    AstroTotals* dtot = reinterpret_cast<AstroTotals*>(parts + reduce_blocks(sz.n_astro));
+    AS_TRY(astro_totals(st_.Ca.get(), st_.ever_active.get(), sz.n_astro, bio_.SIC_th, parts, dtot, stream_));
+    AstroTotals at{};
+    AS_CUDA(cudaMemcpyAsync(&at, dtot, sizeof(at), cudaMemcpyDeviceToHost, stream_));
     AS_CUDA(cudaStreamSynchronize(stream_));
-    u32 engaged = 0;
-    for (unsigned char v : ea) engaged += v;
-    out.mean_ca = mean;
-    out.active_astro = active;
-    out.engaged_astro = engaged;
+    out.mean_ca = at.mean_ca;
+    out.active_astro = at.active;
+    out.engaged_astro = at.engaged;
     out.sic_th = bio_.SIC_th;
     out.build_seconds = net_.build_seconds;
     out.run_seconds = run_seconds_;

@@ -47,6 +47,7 @@ struct StateBuffers {
     DevBuf<unsigned char> sic_last_raw;   // [n_astro] real
     DevBuf<u32> counts;            // spikes per step
     DevBuf<u32> raster;            // [raster_steps][words]
+    DevBuf<unsigned char> reduce_raw;  // summary reduction partials + totals
 };
 
 class Simulation {
