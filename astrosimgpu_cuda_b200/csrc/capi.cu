@@ -8,7 +8,10 @@
 #include <new>
 #include <string>
 
+#include <mutex>
+
 #include "../../include/astrosim.h"
+#include "reduce.cuh"
 #include "sim.cuh"
 
 struct astrosim_handle {
@@ -167,3 +170,59 @@ int astrosim_device_info(int device, char* name, size_t name_cap, int* major, in
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- allocation-free summary reduction
+namespace {
+
+constexpr astrosim::u32 kNoAllocPartials = 4096;
+static_assert(static_cast<unsigned long long>(kNoAllocPartials) * astrosim::kReduceItemsPerBlock ==
+                  ASTROSIM_NOALLOC_MAX_ASTRO,
+              "ASTROSIM_NOALLOC_MAX_ASTRO must match the scratch array");
+static_assert(sizeof(astrosim_astro_totals) == sizeof(astrosim::AstroTotals), "totals layout");
+
+// Scratch of astrosim_astro_totals_noalloc: 4096 partial sums (64 KB) in the device
+// image of every GPU that loads the library.  In host code this name is only a
+// stand-in for the symbol; the device address comes from cudaGetSymbolAddress.
+static __device__ __align__(256) astrosim::AstroPartial g_noalloc_partials[kNoAllocPartials];
+
+constexpr int kMaxDevices = 128;
+std::mutex g_noalloc_mu;
+astrosim::AstroPartial* g_noalloc_addr[kMaxDevices] = {};
+
+}  // namespace
+
+extern "C" int astrosim_astro_totals_noalloc(const double* ca, const unsigned char* engaged, uint32_t n_astro,
+                                             double sic_th, astrosim_astro_totals* out, void* stream) {
+    if (!out) return fail(ASTROSIM_ERR_INVALID_ARG, "null output pointer");
+    if (n_astro > 0 && (!ca || !engaged)) return fail(ASTROSIM_ERR_INVALID_ARG, "null input pointer");
+    if (n_astro > ASTROSIM_NOALLOC_MAX_ASTRO)
+        return fail(ASTROSIM_ERR_INVALID_ARG,
+                    "n_astro exceeds ASTROSIM_NOALLOC_MAX_ASTRO (8388608), the capacity of the static scratch");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ASTROSIM_ERR_NO_DEVICE, "no current CUDA device");
+    }
+    if (dev < 0 || dev >= kMaxDevices) return fail(ASTROSIM_ERR_INVALID_ARG, "device ordinal too large");
+    astrosim::AstroPartial* scratch = nullptr;
+    {
+        // once per device, with that device current: the device address of the scratch
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_addr[dev]) {
+            void* p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+            if (e != cudaSuccess || !p) {
+                cudaGetLastError();
+                return fail(ASTROSIM_ERR_CUDA, "cudaGetSymbolAddress of the no-alloc scratch failed");
+            }
+            g_noalloc_addr[dev] = static_cast<astrosim::AstroPartial*>(p);
+        }
+        scratch = g_noalloc_addr[dev];
+    }
+    return guarded([&] {
+        return astrosim::astro_totals(ca, engaged, n_astro, sic_th, scratch,
+                                      reinterpret_cast<astrosim::AstroTotals*>(out),
+                                      static_cast<cudaStream_t>(stream));
+    });
+}

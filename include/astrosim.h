@@ -201,6 +201,48 @@ int astrosim_last_step_ms(astrosim_handle* h, double* ms);
  */
 int astrosim_device_info(int device, char* name, size_t name_cap, int* major, int* minor);
 
+/*
+ * Astrocyte summary totals over caller-provided device arrays (the layout the
+ * library reduces internally for astrosim_summary).
+ */
+typedef struct astrosim_astro_totals {
+    double sum_ca;     /* sum of calcium over all astrocytes */
+    double mean_ca;    /* sum_ca / max(1, n_astro) */
+    uint32_t active;   /* astrocytes with (Ca - sic_th) * 1000 > 1 */
+    uint32_t engaged;  /* astrocytes whose engaged flag is non-zero */
+} astrosim_astro_totals;
+
+/* Largest n_astro astrosim_astro_totals_noalloc accepts (4096 partial sums of 2048 astrocytes). */
+#define ASTROSIM_NOALLOC_MAX_ASTRO 8388608u
+
+/*
+ * The astrocyte summary reduction that allocates nothing.
+ *
+ * No counterpart in the reference: it is an extra entry point of this library.
+ * It runs the same two-pass reduction astrosim_summary uses, on device arrays the
+ * caller owns: `ca` (n_astro doubles), `engaged` (n_astro bytes, non-zero =
+ * engaged) and `out` (one astrosim_astro_totals in device memory), enqueued on
+ * `stream` (a cudaStream_t; NULL = the legacy default stream) without waiting.
+ *
+ * It is for callers that cannot allocate device memory at the point where they
+ * need the totals: applications that hand all device memory to their own pool or
+ * run under a fixed memory budget, and loops that must not enter the CUDA
+ * allocator because cudaMalloc/cudaFree may synchronize the device or stall on
+ * the driver.  Its scratch (the per-block partial sums) is a static array in the
+ * library's device image, 64 KB on every GPU that loads the library, held until
+ * the process exits; that bounds n_astro to ASTROSIM_NOALLOC_MAX_ASTRO, and larger
+ * inputs return ASTROSIM_ERR_INVALID_ARG.
+ *
+ * The first call on a device (with that device current) looks up the scratch
+ * address once; make that first call before any stream capture.  All calls share
+ * the one scratch array: calls that may overlap on the GPU (different streams,
+ * or different host threads) race and must be serialised by the caller.  Each
+ * call writes every partial it reads, so nothing left by an earlier call leaks
+ * into a result.
+ */
+int astrosim_astro_totals_noalloc(const double* ca, const unsigned char* engaged, uint32_t n_astro, double sic_th,
+                                  astrosim_astro_totals* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
