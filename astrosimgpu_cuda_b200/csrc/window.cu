@@ -6,6 +6,10 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <map>
+#include <mutex>
+#include <type_traits>
+#include <utility>
 
 #include "step_kernels.cuh"
 #include "window.cuh"
@@ -94,9 +98,13 @@ __device__ __forceinline__ void pull_row(const u32* __restrict__ rs, const u32* 
     }
 }
 
-template <typename R>
-__global__ void __launch_bounds__(128) window_kernel(RunConsts rc, StepPtrs<R> p, WinPtrs<R> w, i64 win_start,
-                                                     int s_begin, int s_end, int buf, i64 mark, u32 astro_blocks) {
+// MinBlocks is the launch-bounds occupancy target: the autotuner (window_launch)
+// times the instantiated values on the first windows of a run and keeps the fastest.
+// The per-cell arithmetic is the same in every instantiation.
+template <typename R, int MinBlocks>
+__global__ void __launch_bounds__(128, MinBlocks) window_kernel(RunConsts rc, StepPtrs<R> p, WinPtrs<R> w,
+                                                                i64 win_start, int s_begin, int s_end, int buf,
+                                                                i64 mark, u32 astro_blocks) {
     const int prev = buf ^ 1;
     const int W = w.W;
     const bool window_done = s_end == W;
@@ -406,20 +414,59 @@ Status window_setup(const RunConsts& rc, Network& net, bool fp32, WindowState& w
     AS_TRY(ws.sic_win.alloc_zero(2 * nA * ws.W * rb, st));
     AS_TRY(ws.astro_active.alloc_zero(2 * ((nA + 31) / 32), st));
     AS_TRY(ws.mode.alloc_zero(2, st));
+    AS_CUDA(cudaEventCreate(&ws.tune_ev[0]));
+    AS_CUDA(cudaEventCreate(&ws.tune_ev[1]));
     AS_CUDA(cudaStreamSynchronize(st));
     return Status::Ok();
 }
 
 namespace {
+
+// Launch-bounds variants the autotuner chooses from (minimum resident blocks of 128
+// threads per SM): more blocks trade registers (and a few spills) for occupancy.
+constexpr int kVariantsF32[] = {6, 8, 4};
+constexpr int kVariantsF64[] = {4, 6, 3};
+constexpr int kNumVariants = 3;
+constexpr int kTuneRounds = 2;
+
+std::mutex g_tune_mu;
+std::map<std::pair<int, int>, int> g_tuned;  // (precision, log2 size bucket) -> variant
+
+template <typename R>
+void launch_window(int variant, u32 grid, cudaStream_t st, const RunConsts& rc, const StepPtrs<R>& p,
+                   const WinPtrs<R>& w, i64 start, int s0, int s1, int buf, i64 mark, u32 astro_blocks) {
+    constexpr bool f32 = std::is_same<R, float>::value;
+    const int mb = f32 ? kVariantsF32[variant] : kVariantsF64[variant];
+    switch (mb) {
+        case 3: window_kernel<R, 3><<<grid, 128, 0, st>>>(rc, p, w, start, s0, s1, buf, mark, astro_blocks); break;
+        case 4: window_kernel<R, 4><<<grid, 128, 0, st>>>(rc, p, w, start, s0, s1, buf, mark, astro_blocks); break;
+        case 6: window_kernel<R, 6><<<grid, 128, 0, st>>>(rc, p, w, start, s0, s1, buf, mark, astro_blocks); break;
+        default: window_kernel<R, 8><<<grid, 128, 0, st>>>(rc, p, w, start, s0, s1, buf, mark, astro_blocks); break;
+    }
+}
+
 template <typename R>
 Status launch_impl(const RunConsts& rc, StateBuffers& sb, Network& net, WindowState& ws, i64 raster_steps, i64 mark,
-                   i64 first, i64 count, cudaStream_t st, int block) {
+                   i64 first, i64 count, cudaStream_t st) {
+    constexpr bool f32 = std::is_same<R, float>::value;
     StepPtrs<R> p = make_ptrs<R>(sb, net, rc, raster_steps);
     WinPtrs<R> w = win_ptrs<R>(ws, rc);
-    const u32 astro_blocks = ceil_div(rc.n_astro, block);
-    const u32 neuron_blocks = ceil_div(rc.n_neurons, block);
+    const u32 astro_blocks = ceil_div(rc.n_astro, 128);
+    const u32 neuron_blocks = ceil_div(rc.n_neurons, 128);
     const int W = ws.W;
     const u32 push_blocks = std::max<u32>(1, std::min<u32>(148 * 8, ceil_div(ws.push_limit, 8)));
+    int bucket = 0;
+    while ((1ull << bucket) < rc.n_neurons) ++bucket;
+    const std::pair<int, int> key{f32 ? 1 : 0, bucket};
+    if (ws.variant < 0) {
+        if (const char* env = std::getenv("ASTROSIM_WINDOW_VARIANT")) {
+            ws.variant = std::min(kNumVariants - 1, std::max(0, std::atoi(env)));
+        } else {
+            std::lock_guard<std::mutex> lock(g_tune_mu);
+            auto it = g_tuned.find(key);
+            if (it != g_tuned.end()) ws.variant = it->second;
+        }
+    }
     i64 t = first;
     const i64 end = first + count;
     while (t < end) {
@@ -427,9 +474,26 @@ Status launch_impl(const RunConsts& rc, StateBuffers& sb, Network& net, WindowSt
         const int s0 = static_cast<int>(t - k * W);
         const int s1 = static_cast<int>(std::min<i64>(W, end - k * W));
         const int buf = static_cast<int>(k & 1);
-        window_kernel<R><<<astro_blocks + neuron_blocks, block, 0, st>>>(rc, p, w, k * W, s0, s1, buf, mark,
-                                                                          astro_blocks);
+        const bool tuning = ws.variant < 0 && s0 == 0 && s1 == W;
+        const int v = ws.variant >= 0 ? ws.variant : (tuning ? ws.tune_step % kNumVariants : 0);
+        if (tuning) AS_CUDA(cudaEventRecord(ws.tune_ev[0], st));
+        launch_window<R>(v, astro_blocks + neuron_blocks, st, rc, p, w, k * W, s0, s1, buf, mark, astro_blocks);
         AS_CUDA(cudaGetLastError());
+        if (tuning) {
+            AS_CUDA(cudaEventRecord(ws.tune_ev[1], st));
+            AS_CUDA(cudaEventSynchronize(ws.tune_ev[1]));
+            float ms = 0.f;
+            AS_CUDA(cudaEventElapsedTime(&ms, ws.tune_ev[0], ws.tune_ev[1]));
+            ws.tune_ms[v] = std::min(ws.tune_ms[v], ms);  // min over rounds: the first launch also loads the kernel
+            if (++ws.tune_step == kNumVariants * kTuneRounds) {
+                int best = 0;
+                for (int i = 1; i < kNumVariants; ++i)
+                    if (ws.tune_ms[i] < ws.tune_ms[best]) best = i;
+                ws.variant = best;
+                std::lock_guard<std::mutex> lock(g_tune_mu);
+                g_tuned[key] = best;
+            }
+        }
         if (s1 == W) {
             push_kernel<R><<<push_blocks, 256, 0, st>>>(w, rc.n_exc, net.sz.n_inh, rc.n_neurons, rc.n_astro, buf);
             AS_CUDA(cudaGetLastError());
@@ -443,8 +507,8 @@ Status launch_impl(const RunConsts& rc, StateBuffers& sb, Network& net, WindowSt
 Status window_launch(const RunConsts& rc, StateBuffers& sb, Network& net, bool fp32, WindowState& ws,
                      i64 raster_steps, i64 mark_step, i64 first, i64 count, cudaStream_t st, int block) {
     (void)block;
-    if (fp32) return launch_impl<float>(rc, sb, net, ws, raster_steps, mark_step, first, count, st, 128);
-    return launch_impl<double>(rc, sb, net, ws, raster_steps, mark_step, first, count, st, 128);
+    if (fp32) return launch_impl<float>(rc, sb, net, ws, raster_steps, mark_step, first, count, st);
+    return launch_impl<double>(rc, sb, net, ws, raster_steps, mark_step, first, count, st);
 }
 
 }  // namespace astrosim

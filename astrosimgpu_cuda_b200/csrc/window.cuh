@@ -53,6 +53,15 @@ struct WindowState {
     DevBuf<unsigned char> sic_win;            // [2][n_astro][W] real
     DevBuf<u32> astro_active;                 // [2][ceil(n_astro / 32)]
     DevBuf<int> mode;                         // [2]: 0 push, 1 pull
+    // autotuner: launch-bounds variant of window_kernel (-1 while timing the candidates)
+    int variant = -1;
+    int tune_step = 0;
+    float tune_ms[4] = {1e30f, 1e30f, 1e30f, 1e30f};
+    cudaEvent_t tune_ev[2] = {nullptr, nullptr};
+    ~WindowState() {
+        if (tune_ev[0]) cudaEventDestroy(tune_ev[0]);
+        if (tune_ev[1]) cudaEventDestroy(tune_ev[1]);
+    }
 };
 
 Status window_setup(const RunConsts& rc, Network& net, bool fp32, WindowState& ws, cudaStream_t st);

@@ -51,3 +51,15 @@ def test_windowed_dt_quarter_ms(monkeypatch):
     got = run(monkeypatch, "auto", None, (7, 393), **kw)
     for k in STATES + ("counts",):
         np.testing.assert_array_equal(got[k], ref[k], err_msg=k)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_every_launch_variant_is_bit_identical(monkeypatch, precision):
+    kw = dict(n_total=4000, seed=5, pre_ms=20, sim_ms=60, precision=precision)
+    ref = run(monkeypatch, "plain", None, (800,), **kw)
+    for v in (0, 1, 2):
+        monkeypatch.setenv("ASTROSIM_WINDOW_VARIANT", str(v))
+        got = run(monkeypatch, "auto", None, (13, 787), **kw)
+        for k in STATES + ("counts",):
+            np.testing.assert_array_equal(got[k], ref[k], err_msg=f"{k} variant {v}")
+    monkeypatch.delenv("ASTROSIM_WINDOW_VARIANT")
