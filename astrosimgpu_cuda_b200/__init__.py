@@ -66,6 +66,19 @@ def lib():
     L.astrosim_dump_edges.argtypes = [P, C.c_char_p]
     L.astrosim_last_step_ms.argtypes = [P, C.POINTER(C.c_double)]
     L.astrosim_device_info.argtypes = [C.c_int, C.c_char_p, C.c_size_t, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    E = C.c_void_p
+    L.astrosim_ensemble_create.argtypes = [C.POINTER(abi.Config), C.c_uint32, C.POINTER(E)]
+    L.astrosim_ensemble_step.argtypes = [E, C.c_int64]
+    L.astrosim_ensemble_summary.argtypes = [E, C.c_uint32, C.POINTER(abi.Summary)]
+    L.astrosim_ensemble_get_state.argtypes = [E, C.c_uint32, C.c_int, C.POINTER(C.c_double), C.c_size_t]
+    L.astrosim_ensemble_spike_counts.argtypes = [E, C.c_uint32, C.c_int64, C.c_int64, u32p]
+    L.astrosim_ensemble_last_step_ms.argtypes = [E, C.POINTER(C.c_double)]
+    L.astrosim_ensemble_build_seconds.argtypes = [E, C.POINTER(C.c_double)]
+    L.astrosim_ensemble_destroy.argtypes = [E]
+    for name in ("astrosim_ensemble_create", "astrosim_ensemble_step", "astrosim_ensemble_summary",
+                 "astrosim_ensemble_get_state", "astrosim_ensemble_spike_counts", "astrosim_ensemble_last_step_ms",
+                 "astrosim_ensemble_build_seconds", "astrosim_ensemble_destroy"):
+        getattr(L, name).restype = C.c_int
     for name in ("astrosim_create", "astrosim_step", "astrosim_summary", "astrosim_destroy",
                  "astrosim_spike_counts", "astrosim_raster", "astrosim_get_state", "astrosim_get_csr",
                  "astrosim_dump_edges", "astrosim_last_step_ms", "astrosim_device_info"):
@@ -164,6 +177,70 @@ class Simulation:
 
     def dump_edges(self, path):
         check(lib().astrosim_dump_edges(self._h, os.fsencode(path)))
+
+
+class Ensemble:
+    """Many independent networks stepped together (astrosim_ensemble_*)."""
+
+    def __init__(self, cfgs):
+        self.cfgs = list(cfgs)
+        arr = (abi.Config * len(self.cfgs))(*self.cfgs)
+        self._h = C.c_void_p()
+        check(lib().astrosim_ensemble_create(arr, len(self.cfgs), C.byref(self._h)))
+        self.sizes = [scaling(c.n_total) for c in self.cfgs]
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().astrosim_ensemble_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self):
+        return len(self.cfgs)
+
+    def step(self, n):
+        check(lib().astrosim_ensemble_step(self._h, int(n)))
+
+    def summary(self, i):
+        s = abi.Summary()
+        check(lib().astrosim_ensemble_summary(self._h, i, C.byref(s)))
+        return s.as_dict()
+
+    def state(self, i, name):
+        n_exc, n_inh, n_astro, _ = self.sizes[i]
+        n = n_astro if name in abi.ASTRO_STATES else n_exc + n_inh
+        out = np.empty(n, dtype=np.float64)
+        check(lib().astrosim_ensemble_get_state(self._h, i, abi.STATE[name],
+                                                out.ctypes.data_as(C.POINTER(C.c_double)), n))
+        return out
+
+    def spike_counts(self, i, first=0, n=None):
+        if n is None:
+            n = self.summary(i)["steps_done"] - first
+        out = np.empty(n, dtype=np.uint32)
+        check(lib().astrosim_ensemble_spike_counts(self._h, i, first, n, _u32p(out)))
+        return out
+
+    def last_step_ms(self):
+        ms = C.c_double()
+        check(lib().astrosim_ensemble_last_step_ms(self._h, C.byref(ms)))
+        return ms.value
+
+    def build_seconds(self):
+        s = C.c_double()
+        check(lib().astrosim_ensemble_build_seconds(self._h, C.byref(s)))
+        return s.value
 
 
 def rate_hz(spikes, n_neurons, ms):

@@ -11,11 +11,16 @@
 #include <mutex>
 
 #include "../../include/astrosim.h"
+#include "ensemble.cuh"
 #include "reduce.cuh"
 #include "sim.cuh"
 
 struct astrosim_handle {
     astrosim::Simulation sim;
+};
+
+struct astrosim_ensemble {
+    astrosim::Ensemble ens;
 };
 
 namespace {
@@ -147,6 +152,71 @@ int astrosim_dump_edges(astrosim_handle* h, const char* path) {
 int astrosim_last_step_ms(astrosim_handle* h, double* ms) {
     if (!h || !ms) return fail(ASTROSIM_ERR_INVALID_ARG, "null argument");
     return guarded([&] { return h->sim.last_step_ms(ms); });
+}
+
+int astrosim_ensemble_create(const astrosim_config* cfgs, uint32_t n_networks, astrosim_ensemble** out) {
+    if (!cfgs || !out) return fail(ASTROSIM_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    for (uint32_t i = 0; i < n_networks; ++i) {
+        if (cfgs[i].struct_size != sizeof(astrosim_config))
+            return fail(ASTROSIM_ERR_INVALID_ARG, "astrosim_config.struct_size mismatch");
+        for (int r : cfgs[i].reserved)
+            if (r != 0) return fail(ASTROSIM_ERR_INVALID_ARG, "astrosim_config.reserved must be zero");
+    }
+    astrosim_ensemble* e = nullptr;
+    try {
+        e = new astrosim_ensemble();
+    } catch (...) {
+        return fail(ASTROSIM_ERR_OUT_OF_MEMORY, "host allocation failed");
+    }
+    const int rc = guarded([&] { return e->ens.create(cfgs, n_networks); });
+    if (rc != ASTROSIM_OK) {
+        const std::string msg = g_last_error;
+        delete e;
+        g_last_error = msg;
+        return rc;
+    }
+    *out = e;
+    return ASTROSIM_OK;
+}
+
+int astrosim_ensemble_step(astrosim_ensemble* e, int64_t n_steps) {
+    if (!e) return fail(ASTROSIM_ERR_INVALID_ARG, "null ensemble");
+    return guarded([&] { return e->ens.step(n_steps); });
+}
+
+int astrosim_ensemble_summary(astrosim_ensemble* e, uint32_t index, astrosim_summary_t* out) {
+    if (!e || !out) return fail(ASTROSIM_ERR_INVALID_ARG, "null argument");
+    return guarded([&] { return e->ens.summary(index, *out); });
+}
+
+int astrosim_ensemble_get_state(astrosim_ensemble* e, uint32_t index, int which, double* dst, size_t count) {
+    if (!e) return fail(ASTROSIM_ERR_INVALID_ARG, "null ensemble");
+    return guarded([&] { return e->ens.get_state(index, which, dst, count); });
+}
+
+int astrosim_ensemble_spike_counts(astrosim_ensemble* e, uint32_t index, int64_t first_step, int64_t n,
+                                   uint32_t* counts) {
+    if (!e) return fail(ASTROSIM_ERR_INVALID_ARG, "null ensemble");
+    return guarded([&] { return e->ens.spike_counts(index, first_step, n, counts); });
+}
+
+int astrosim_ensemble_last_step_ms(astrosim_ensemble* e, double* ms) {
+    if (!e || !ms) return fail(ASTROSIM_ERR_INVALID_ARG, "null argument");
+    return guarded([&] { return e->ens.last_step_ms(ms); });
+}
+
+int astrosim_ensemble_build_seconds(astrosim_ensemble* e, double* seconds) {
+    if (!e || !seconds) return fail(ASTROSIM_ERR_INVALID_ARG, "null argument");
+    *seconds = e->ens.build_seconds();
+    g_last_error.clear();
+    return ASTROSIM_OK;
+}
+
+int astrosim_ensemble_destroy(astrosim_ensemble* e) {
+    delete e;
+    g_last_error.clear();
+    return ASTROSIM_OK;
 }
 
 int astrosim_device_info(int device, char* name, size_t name_cap, int* major, int* minor) {

@@ -1,0 +1,396 @@
+// ensemble.cu -- batched stepping of many independent networks (see ensemble.cuh).
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstring>
+#include <thread>
+
+#include "ensemble.cuh"
+#include "window_kernels.cuh"
+
+namespace astrosim {
+
+namespace {
+
+template <typename R>
+struct alignas(16) NetDesc {
+    RunConsts rc;
+    StepPtrs<R> p;
+    WinPtrs<R> w;
+    i64 mark;  // last step of the pre-run (src/astrosim_fused.cu:1066)
+};
+
+constexpr int kEnsVariants[] = {6, 8, 4};  // launch-bounds minimum blocks, as the single-network engine
+constexpr int kEnsNumVariants = 3;
+constexpr int kEnsTuneRounds = 2;
+constexpr int kGraphWindows = 10;
+constexpr u32 kPushBlocksPerNet = 4;
+
+template <typename R, int MB>
+__global__ void __launch_bounds__(128, MB) ens_window_kernel(const NetDesc<R>* __restrict__ descs,
+                                                             const u32* __restrict__ tile_net,
+                                                             const u32* __restrict__ tile_blk,
+                                                             const i64* __restrict__ win,
+                                                             const i64* __restrict__ stop, int W) {
+    __shared__ __align__(16) unsigned char smem[sizeof(NetDesc<R>)];
+    const u32 net = tile_net[blockIdx.x];
+    const i64 k = win[net];
+    const i64 start = k * W;
+    const i64 end = stop[net];
+    if (start >= end) return;  // finished or retired network: the whole block leaves
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(descs + net);
+        uint4* dst = reinterpret_cast<uint4*>(smem);
+        for (u32 i = threadIdx.x; i < sizeof(NetDesc<R>) / sizeof(uint4); i += blockDim.x) dst[i] = src[i];
+    }
+    __syncthreads();
+    const NetDesc<R>& d = *reinterpret_cast<const NetDesc<R>*>(smem);
+    const int s_end = static_cast<int>(end - start < W ? end - start : W);
+    const u32 tb = tile_blk[blockIdx.x];
+    window_cells<R>(d.rc, d.p, d.w, start, 0, s_end, static_cast<int>(k & 1), d.mark, tb & 0x7FFFFFFFu,
+                    (tb >> 31) != 0);
+}
+
+template <typename R>
+__global__ void ens_push_kernel(const NetDesc<R>* __restrict__ descs, const i64* __restrict__ win,
+                                const i64* __restrict__ stop, int W) {
+    const u32 net = blockIdx.y;
+    const i64 k = win[net];
+    if (k * W + W > stop[net]) return;  // the window did not complete: no window follows it
+    const NetDesc<R>& d = descs[net];
+    push_cells<R>(d.w, d.rc.n_exc, d.rc.n_neurons - d.rc.n_exc, d.rc.n_neurons, d.rc.n_astro,
+                  static_cast<int>(k & 1), blockIdx.x, gridDim.x);
+}
+
+__global__ void ens_advance_kernel(i64* win, const i64* stop, u32 n, int W) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && win[i] * W < stop[i]) win[i] += 1;
+}
+
+template <typename R>
+void launch_ens_window(int v, u32 grid, cudaStream_t st, const NetDesc<R>* d, const u32* tn, const u32* tb,
+                       const i64* win, const i64* stop, int W) {
+    switch (kEnsVariants[v]) {
+        case 4: ens_window_kernel<R, 4><<<grid, 128, 0, st>>>(d, tn, tb, win, stop, W); break;
+        case 8: ens_window_kernel<R, 8><<<grid, 128, 0, st>>>(d, tn, tb, win, stop, W); break;
+        default: ens_window_kernel<R, 6><<<grid, 128, 0, st>>>(d, tn, tb, win, stop, W); break;
+    }
+}
+
+template <typename R>
+Status build_descs(std::vector<std::unique_ptr<Simulation>>& nets, DevBuf<unsigned char>& descs, cudaStream_t st) {
+    std::vector<NetDesc<R>> h(nets.size());
+    std::memset(static_cast<void*>(h.data()), 0, h.size() * sizeof(NetDesc<R>));
+    for (size_t i = 0; i < nets.size(); ++i) {
+        Simulation* s = nets[i].get();
+        if (!s) continue;
+        const RunConsts& rc = s->consts();
+        h[i].rc = rc;
+        h[i].p = make_ptrs<R>(s->state_buffers(), s->network(), rc, s->raster_steps());
+        h[i].w = win_ptrs<R>(*s->window_state(), rc);
+        h[i].mark = s->pre_steps() == 0 ? 0 : s->pre_steps() - 1;
+    }
+    AS_TRY(descs.alloc(std::max<size_t>(1, h.size()) * sizeof(NetDesc<R>)));
+    if (!h.empty())
+        AS_CUDA(cudaMemcpyAsync(descs.get(), h.data(), h.size() * sizeof(NetDesc<R>), cudaMemcpyHostToDevice, st));
+    AS_CUDA(cudaStreamSynchronize(st));
+    return Status::Ok();
+}
+
+}  // namespace
+
+Ensemble::~Ensemble() {
+    if (graph_) cudaGraphExecDestroy(graph_);
+    if (ev0_) cudaEventDestroy(ev0_);
+    if (ev1_) cudaEventDestroy(ev1_);
+    nets_.clear();
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+Status Ensemble::init_empty(bool fp32, int window, int device) {
+    fp32_ = fp32;
+    W_ = window;
+    device_ = device;
+    AS_CUDA(cudaSetDevice(device_));
+    AS_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    AS_CUDA(cudaEventCreate(&ev0_));
+    AS_CUDA(cudaEventCreate(&ev1_));
+    dirty_ = true;
+    return Status::Ok();
+}
+
+Status Ensemble::create(const astrosim_config* cfgs, u32 n) {
+    if (!cfgs || n == 0) return make_error(ASTROSIM_ERR_INVALID_ARG, "an ensemble needs at least one network");
+    for (u32 i = 1; i < n; ++i) {
+        if (cfgs[i].dt != cfgs[0].dt || cfgs[i].substeps != cfgs[0].substeps ||
+            cfgs[i].precision != cfgs[0].precision || cfgs[i].device != cfgs[0].device)
+            return make_error(ASTROSIM_ERR_INVALID_ARG,
+                              "ensemble networks must share dt, substeps, precision and device (network %u differs)", i);
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    nets_.resize(n);
+    std::vector<Status> st(n);
+    std::atomic<u32> next{0};
+    const u32 workers = std::min<u32>(n, std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
+    auto work = [&] {
+        for (u32 i = next++; i < n; i = next++) {
+            auto s = std::make_unique<Simulation>();
+            st[i] = s->create(cfgs[i]);
+            nets_[i] = std::move(s);
+        }
+    };
+    // networks are built concurrently, each on its own stream
+    std::vector<std::thread> pool;
+    for (u32 t = 1; t < workers; ++t) pool.emplace_back(work);
+    work();
+    for (auto& th : pool) th.join();
+    for (u32 i = 0; i < n; ++i)
+        if (!st[i].ok()) return make_error(st[i].code, "network %u: %s", i, st[i].msg.c_str());
+    for (u32 i = 0; i < n; ++i)
+        if (!nets_[i]->windowed() || nets_[i]->consts().d_e != nets_[0]->consts().d_e)
+            return make_error(ASTROSIM_ERR_UNSUPPORTED, "ensemble networks need the windowed engine with one window");
+    AS_TRY(init_empty(cfgs[0].precision == ASTROSIM_PRECISION_FP32, nets_[0]->consts().d_e, cfgs[0].device));
+    win_host_.assign(n, 0);
+    AS_TRY(win_.alloc_zero(n, stream_));
+    std::vector<i64> stops(n);
+    for (u32 i = 0; i < n; ++i) stops[i] = nets_[i]->total_steps();
+    AS_TRY(stop_.alloc(n));
+    AS_CUDA(cudaMemcpyAsync(stop_.get(), stops.data(), n * sizeof(i64), cudaMemcpyHostToDevice, stream_));
+    AS_TRY(rebuild());
+    build_seconds_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return Status::Ok();
+}
+
+Status Ensemble::rebuild() {
+    AS_CUDA(cudaSetDevice(device_));
+    if (fp32_) AS_TRY(build_descs<float>(nets_, descs_, stream_));
+    else AS_TRY(build_descs<double>(nets_, descs_, stream_));
+    std::vector<u32> tn, tb;
+    for (u32 i = 0; i < nets_.size(); ++i) {
+        if (!nets_[i]) continue;
+        const RunConsts& rc = nets_[i]->consts();
+        for (u32 b = 0; b < ceil_div(rc.n_astro, 128); ++b) {
+            tn.push_back(i);
+            tb.push_back(b | 0x80000000u);
+        }
+        for (u32 b = 0; b < ceil_div(rc.n_neurons, 128); ++b) {
+            tn.push_back(i);
+            tb.push_back(b);
+        }
+    }
+    n_tiles_ = static_cast<u32>(tn.size());
+    AS_TRY(tile_net_.alloc(std::max<size_t>(1, tn.size())));
+    AS_TRY(tile_blk_.alloc(std::max<size_t>(1, tb.size())));
+    if (!tn.empty()) {
+        AS_CUDA(cudaMemcpyAsync(tile_net_.get(), tn.data(), tn.size() * sizeof(u32), cudaMemcpyHostToDevice, stream_));
+        AS_CUDA(cudaMemcpyAsync(tile_blk_.get(), tb.data(), tb.size() * sizeof(u32), cudaMemcpyHostToDevice, stream_));
+    }
+    AS_CUDA(cudaStreamSynchronize(stream_));
+    if (graph_) {
+        cudaGraphExecDestroy(graph_);
+        graph_ = nullptr;
+    }
+    dirty_ = false;
+    return Status::Ok();
+}
+
+Status Ensemble::capture_graph() {
+    if (graph_) return Status::Ok();
+    const u32 n = static_cast<u32>(nets_.size());
+    cudaGraph_t g = nullptr;
+    AS_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < kGraphWindows; ++k) {
+        if (fp32_) {
+            launch_ens_window<float>(variant_, n_tiles_, stream_, reinterpret_cast<const NetDesc<float>*>(descs_.get()),
+                                     tile_net_.get(), tile_blk_.get(), win_.get(), stop_.get(), W_);
+            ens_push_kernel<float><<<dim3(kPushBlocksPerNet, n), 256, 0, stream_>>>(
+                reinterpret_cast<const NetDesc<float>*>(descs_.get()), win_.get(), stop_.get(), W_);
+        } else {
+            launch_ens_window<double>(variant_, n_tiles_, stream_,
+                                      reinterpret_cast<const NetDesc<double>*>(descs_.get()), tile_net_.get(),
+                                      tile_blk_.get(), win_.get(), stop_.get(), W_);
+            ens_push_kernel<double><<<dim3(kPushBlocksPerNet, n), 256, 0, stream_>>>(
+                reinterpret_cast<const NetDesc<double>*>(descs_.get()), win_.get(), stop_.get(), W_);
+        }
+        ens_advance_kernel<<<ceil_div(n, 256), 256, 0, stream_>>>(win_.get(), stop_.get(), n, W_);
+    }
+    const cudaError_t e = cudaStreamEndCapture(stream_, &g);
+    if (e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return cuda_status(e, "cudaStreamEndCapture", __FILE__, __LINE__);
+    }
+    const cudaError_t e2 = cudaGraphInstantiate(&graph_, g, 0);
+    cudaGraphDestroy(g);
+    if (e2 != cudaSuccess) {
+        graph_ = nullptr;
+        return cuda_status(e2, "cudaGraphInstantiate", __FILE__, __LINE__);
+    }
+    graph_windows_ = kGraphWindows;
+    return Status::Ok();
+}
+
+Status Ensemble::advance_windows(i64 windows) {
+    AS_CUDA(cudaSetDevice(device_));
+    if (dirty_) AS_TRY(rebuild());
+    const u32 n = static_cast<u32>(nets_.size());
+    if (n == 0 || n_tiles_ == 0 || windows <= 0) return Status::Ok();
+    const auto t0 = std::chrono::steady_clock::now();
+    AS_CUDA(cudaEventRecord(ev0_, stream_));
+    i64 done = 0;
+    auto one_window = [&](int v) -> Status {
+        if (fp32_) {
+            launch_ens_window<float>(v, n_tiles_, stream_, reinterpret_cast<const NetDesc<float>*>(descs_.get()),
+                                     tile_net_.get(), tile_blk_.get(), win_.get(), stop_.get(), W_);
+            ens_push_kernel<float><<<dim3(kPushBlocksPerNet, n), 256, 0, stream_>>>(
+                reinterpret_cast<const NetDesc<float>*>(descs_.get()), win_.get(), stop_.get(), W_);
+        } else {
+            launch_ens_window<double>(v, n_tiles_, stream_, reinterpret_cast<const NetDesc<double>*>(descs_.get()),
+                                      tile_net_.get(), tile_blk_.get(), win_.get(), stop_.get(), W_);
+            ens_push_kernel<double><<<dim3(kPushBlocksPerNet, n), 256, 0, stream_>>>(
+                reinterpret_cast<const NetDesc<double>*>(descs_.get()), win_.get(), stop_.get(), W_);
+        }
+        ens_advance_kernel<<<ceil_div(n, 256), 256, 0, stream_>>>(win_.get(), stop_.get(), n, W_);
+        AS_CUDA(cudaGetLastError());
+        return Status::Ok();
+    };
+    // autotune the launch-bounds variant on the first windows (results do not depend on it)
+    while (variant_ < 0 && done < windows) {
+        const int v = tune_step_ % kEnsNumVariants;
+        cudaEvent_t a = nullptr, b = nullptr;
+        AS_CUDA(cudaEventCreate(&a));
+        AS_CUDA(cudaEventCreate(&b));
+        AS_CUDA(cudaEventRecord(a, stream_));
+        Status s = one_window(v);
+        AS_CUDA(cudaEventRecord(b, stream_));
+        AS_CUDA(cudaEventSynchronize(b));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        AS_TRY(s);
+        tune_ms_[v] = std::min(tune_ms_[v], ms);
+        ++done;
+        if (++tune_step_ == kEnsNumVariants * kEnsTuneRounds) {
+            int best = 0;
+            for (int i = 1; i < kEnsNumVariants; ++i)
+                if (tune_ms_[i] < tune_ms_[best]) best = i;
+            variant_ = best;
+        }
+    }
+    if (done < windows) {
+        AS_TRY(capture_graph());
+        while (windows - done >= graph_windows_) {
+            AS_CUDA(cudaGraphLaunch(graph_, stream_));
+            done += graph_windows_;
+        }
+        while (done < windows) {
+            AS_TRY(one_window(variant_));
+            ++done;
+        }
+    }
+    AS_CUDA(cudaEventRecord(ev1_, stream_));
+    have_events_ = true;
+    AS_CUDA(cudaStreamSynchronize(stream_));
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    // every unfinished network advanced one window per window launched
+    for (u32 i = 0; i < n; ++i) {
+        if (!nets_[i]) continue;
+        const i64 before = nets_[i]->steps_done();
+        const i64 after = std::min<i64>(nets_[i]->total_steps(), (win_host_[i] + windows) * W_);
+        win_host_[i] = std::min<i64>(win_host_[i] + windows, (nets_[i]->total_steps() + W_ - 1) / W_);
+        if (after > before) nets_[i]->note_external_steps(after - before, secs);
+    }
+    return Status::Ok();
+}
+
+Status Ensemble::step(i64 n_steps) {
+    if (n_steps < 0) return make_error(ASTROSIM_ERR_INVALID_ARG, "n_steps must be >= 0");
+    if (n_steps % W_ != 0)
+        return make_error(ASTROSIM_ERR_INVALID_ARG, "ensemble steps come in whole windows of %d steps", W_);
+    AS_TRY(advance_windows(n_steps / W_));
+    steps_done_ += n_steps;
+    return Status::Ok();
+}
+
+i64 Ensemble::net_steps_done(u32 i) const { return nets_[i] ? nets_[i]->steps_done() : 0; }
+
+Status Ensemble::summary(u32 i, astrosim_summary_t& out) {
+    if (!active(i)) return make_error(ASTROSIM_ERR_INVALID_ARG, "no network %u", i);
+    AS_CUDA(cudaSetDevice(device_));
+    AS_CUDA(cudaStreamSynchronize(stream_));
+    return nets_[i]->summary(out);
+}
+
+Status Ensemble::get_state(u32 i, int which, double* dst, size_t count) {
+    if (!active(i)) return make_error(ASTROSIM_ERR_INVALID_ARG, "no network %u", i);
+    AS_CUDA(cudaStreamSynchronize(stream_));
+    return nets_[i]->get_state(which, dst, count);
+}
+
+Status Ensemble::spike_counts(u32 i, i64 first, i64 n, u32* dst) {
+    if (!active(i)) return make_error(ASTROSIM_ERR_INVALID_ARG, "no network %u", i);
+    AS_CUDA(cudaStreamSynchronize(stream_));
+    return nets_[i]->spike_counts(first, n, dst);
+}
+
+Status Ensemble::last_step_ms(double* ms) {
+    if (!have_events_) return make_error(ASTROSIM_ERR_STATE, "no step has run yet");
+    AS_CUDA(cudaEventSynchronize(ev1_));
+    float f = 0.f;
+    AS_CUDA(cudaEventElapsedTime(&f, ev0_, ev1_));
+    *ms = f;
+    return Status::Ok();
+}
+
+Status Ensemble::add(std::unique_ptr<Simulation> sim) {
+    if (!sim || !sim->windowed() || sim->consts().d_e != W_ || sim->fp32() != fp32_)
+        return make_error(ASTROSIM_ERR_INVALID_ARG, "network does not match the ensemble's window or precision");
+    AS_CUDA(cudaSetDevice(device_));
+    AS_CUDA(cudaStreamSynchronize(stream_));
+    AS_CUDA(cudaStreamSynchronize(sim->stream()));
+    // reuse a retired slot when one is free
+    u32 slot = static_cast<u32>(nets_.size());
+    for (u32 i = 0; i < nets_.size(); ++i)
+        if (!nets_[i]) {
+            slot = i;
+            break;
+        }
+    const i64 stop = sim->total_steps();
+    if (slot == nets_.size()) {
+        nets_.push_back(std::move(sim));
+        win_host_.push_back(0);
+        DevBuf<i64> nw, ns;
+        AS_TRY(nw.alloc(nets_.size()));
+        AS_TRY(ns.alloc(nets_.size()));
+        if (slot > 0) {
+            AS_CUDA(cudaMemcpyAsync(nw.get(), win_.get(), slot * sizeof(i64), cudaMemcpyDeviceToDevice, stream_));
+            AS_CUDA(cudaMemcpyAsync(ns.get(), stop_.get(), slot * sizeof(i64), cudaMemcpyDeviceToDevice, stream_));
+        }
+        win_ = std::move(nw);
+        stop_ = std::move(ns);
+    } else {
+        nets_[slot] = std::move(sim);
+        win_host_[slot] = 0;
+    }
+    const i64 zero = 0;
+    AS_CUDA(cudaMemcpyAsync(win_.get() + slot, &zero, sizeof(i64), cudaMemcpyHostToDevice, stream_));
+    AS_CUDA(cudaMemcpyAsync(stop_.get() + slot, &stop, sizeof(i64), cudaMemcpyHostToDevice, stream_));
+    AS_CUDA(cudaStreamSynchronize(stream_));
+    dirty_ = true;
+    return Status::Ok();
+}
+
+Status Ensemble::retire(u32 i) {
+    if (!active(i)) return make_error(ASTROSIM_ERR_INVALID_ARG, "no network %u", i);
+    AS_CUDA(cudaSetDevice(device_));
+    AS_CUDA(cudaStreamSynchronize(stream_));
+    const i64 zero = 0;
+    AS_CUDA(cudaMemcpyAsync(stop_.get() + i, &zero, sizeof(i64), cudaMemcpyHostToDevice, stream_));
+    AS_CUDA(cudaStreamSynchronize(stream_));
+    nets_[i].reset();
+    dirty_ = true;
+    return Status::Ok();
+}
+
+}  // namespace astrosim

@@ -66,6 +66,25 @@ public:
     const Sizes& sizes() const { return net_.sz; }
     i64 steps_done() const { return steps_done_; }
 
+    // Access for the batched engine (ensemble.cu), which steps many simulations'
+    // windowed state with shared launches.
+    const RunConsts& consts() const { return rc_; }
+    StateBuffers& state_buffers() { return st_; }
+    Network& network() { return net_; }
+    WindowState* window_state() { return win_; }
+    bool fp32() const { return fp32_; }
+    bool windowed() const { return windowed_; }
+    i64 pre_steps() const { return pre_steps_; }
+    i64 total_steps() const { return total_steps_; }
+    i64 raster_steps() const { return cfg_.raster_steps; }
+    cudaStream_t stream() const { return stream_; }
+    const astrosim_config& config() const { return cfg_; }
+    Status reserve_steps(i64 n) { return ensure_counts(n); }
+    void note_external_steps(i64 n, double seconds) {
+        steps_done_ += n;
+        run_seconds_ += seconds;
+    }
+
 private:
     Status launch_steps(i64 first, i64 count);
     Status ensure_counts(i64 steps);

@@ -11,92 +11,11 @@
 #include <type_traits>
 #include <utility>
 
-#include "step_kernels.cuh"
-#include "window.cuh"
+#include "window_kernels.cuh"
 
 namespace astrosim {
 
 namespace {
-
-template <typename R>
-struct WinPtrs {
-    u32 *nin_cnt, *ain_cnt;          // [2][n]
-    Deposit<R> *nin_ent, *ain_ent;   // [2][n][kInboxSlots]
-    u32* spk_word;                   // [2][n_neurons]
-    R* spk_val;                      // [2][W][n_neurons]
-    u32* spk_list;                   // [2][cap]
-    u32* spk_count;                  // [2]
-    R* sic_win;                      // [2][n_astro][W]
-    u32* astro_active;               // [2][astro_words]
-    int* mode;                       // [2]
-    const u32 *fe_rs, *fe_dst, *fi_rs, *fi_dst, *fa_rs, *fa_astro, *fa_pos;
-    u32 cap, push_limit, astro_words;
-    int W;
-};
-
-template <typename R>
-WinPtrs<R> win_ptrs(WindowState& ws, const RunConsts& rc) {
-    WinPtrs<R> w{};
-    w.nin_cnt = ws.nin_cnt.get();
-    w.ain_cnt = ws.ain_cnt.get();
-    w.nin_ent = reinterpret_cast<Deposit<R>*>(ws.nin_ent.get());
-    w.ain_ent = reinterpret_cast<Deposit<R>*>(ws.ain_ent.get());
-    w.spk_word = ws.spk_word.get();
-    w.spk_val = reinterpret_cast<R*>(ws.spk_val.get());
-    w.spk_list = ws.spk_list.get();
-    w.spk_count = ws.spk_count.get();
-    w.sic_win = reinterpret_cast<R*>(ws.sic_win.get());
-    w.astro_active = ws.astro_active.get();
-    w.mode = ws.mode.get();
-    w.fe_rs = ws.fwd.exc_rs.get();
-    w.fe_dst = ws.fwd.exc_dst.get();
-    w.fi_rs = ws.fwd.inh_rs.get();
-    w.fi_dst = ws.fwd.inh_dst.get();
-    w.fa_rs = ws.fwd.e2a_rs.get();
-    w.fa_astro = ws.fwd.e2a_astro.get();
-    w.fa_pos = ws.fwd.e2a_pos.get();
-    w.cap = ws.push_limit + 1;
-    w.push_limit = ws.push_limit;
-    w.astro_words = (rc.n_astro + 31) / 32;
-    w.W = ws.W;
-    return w;
-}
-
-// Sorts deposits by (step, kind, key): the order in which the reference's dense
-// gather meets them (row order within one step and kind).
-template <typename R>
-__device__ __forceinline__ void sort_deposits(Deposit<R>* d, int n) {
-    for (int i = 1; i < n; ++i) {
-        const Deposit<R> x = d[i];
-        const unsigned long long kx = (static_cast<unsigned long long>(x.meta) << 32) | x.key;
-        int k = i - 1;
-        while (k >= 0 && ((static_cast<unsigned long long>(d[k].meta) << 32) | d[k].key) > kx) {
-            d[k + 1] = d[k];
-            --k;
-        }
-        d[k + 1] = x;
-    }
-}
-
-// Per-step sums of one CSR row against the previous window's spike words, in row
-// order (the exact fallback when deposits are not available).
-template <typename R>
-__device__ __forceinline__ void pull_row(const u32* __restrict__ rs, const u32* __restrict__ src, u32 row,
-                                         const u32* __restrict__ words, const R* __restrict__ vals, u64 n_neurons,
-                                         int s0, int s1, R* acc) {
-    const u32 k1 = rs[row + 1];
-    for (u32 k = rs[row]; k < k1; ++k) {
-        const u32 s = src[k];
-        u32 wd = words[s];
-        if (!wd) continue;
-        wd &= ((s1 >= 32 ? 0xFFFFFFFFu : ((1u << s1) - 1u)) & ~((1u << s0) - 1u));
-        while (wd) {
-            const int b = __ffs(wd) - 1;
-            wd &= wd - 1;
-            acc[b] += vals[static_cast<u64>(b) * n_neurons + s];
-        }
-    }
-}
 
 // MinBlocks is the launch-bounds occupancy target: the autotuner (window_launch)
 // times the instantiated values on the first windows of a run and keeps the fastest.
@@ -105,210 +24,14 @@ template <typename R, int MinBlocks>
 __global__ void __launch_bounds__(128, MinBlocks) window_kernel(RunConsts rc, StepPtrs<R> p, WinPtrs<R> w,
                                                                 i64 win_start, int s_begin, int s_end, int buf,
                                                                 i64 mark, u32 astro_blocks) {
-    const int prev = buf ^ 1;
-    const int W = w.W;
-    const bool window_done = s_end == W;
-    const bool pull = w.mode[buf] != 0;
-    if (blockIdx.x < astro_blocks) {
-        // ------------------------------------------------------------ astrocytes
-        const u32 a = blockIdx.x * blockDim.x + threadIdx.x;
-        const bool valid = a < rc.n_astro;
-        bool any_active = false;
-        if (valid) {
-            AstroRegs<R> s{p.Ca[a], p.IP3[a], p.h[a], p.Ca_tot[a], p.IP3_0[a], p.tau_IP3[a], p.delta_IP3[a]};
-            R acc[kMaxWindow];
-            const u64 slot_base = (static_cast<u64>(buf) * rc.n_astro + a);
-            const u32 c = w.ain_cnt[slot_base];
-            const bool ip3_input = pull || c > 0;
-            if (ip3_input)
-                for (int i = 0; i < W; ++i) acc[i] = static_cast<R>(0.0);
-            if (pull || c > kInboxSlots) {
-                pull_row<R>(p.e2a_rs, p.e2a_src, a, w.spk_word + static_cast<u64>(prev) * rc.n_neurons,
-                            w.spk_val + static_cast<u64>(prev) * W * rc.n_neurons, rc.n_neurons, s_begin, s_end, acc);
-            } else if (c > 0) {
-                Deposit<R> d[kInboxSlots];
-                for (u32 i = 0; i < c; ++i) d[i] = w.ain_ent[slot_base * kInboxSlots + i];
-                sort_deposits<R>(d, static_cast<int>(c));
-                for (u32 i = 0; i < c; ++i) {
-                    const int st = static_cast<int>(d[i].meta & 0xFFu);
-                    if (st >= s_begin && st < s_end) acc[st] += d[i].val;
-                }
-            }
-            if (window_done && c) w.ain_cnt[slot_base] = 0;
-            unsigned char ever = p.ever_active[a];
-            R* out = w.sic_win + (static_cast<u64>(buf) * rc.n_astro + a) * W;
-            R factor = static_cast<R>(0.0);
-            u64 pbase = step_base(rc.seed, kAstroPoissonKey, win_start + s_begin, a);
-            u64 nbase = step_base(rc.seed, kAstroNoiseKey, win_start + s_begin, a);
-            for (int st = s_begin; st < s_end; ++st) {
-                const i64 t = win_start + st;
-                factor = astro_advance_step<R>(rc, s, ip3_input ? acc[st] : static_cast<R>(0.0), a, t, pbase, nbase);
-                pbase += kStepAdvance;
-                nbase += kStepAdvance;
-                out[st] = factor;
-                if (factor > static_cast<R>(0.0)) {
-                    ever = 1;
-                    any_active = true;
-                }
-                if (t == mark) ever = 0;  // end of the pre-run (src/astrosim_fused.cu:1075)
-            }
-            p.Ca[a] = s.Ca;
-            p.IP3[a] = s.IP3;
-            p.h[a] = s.h;
-            p.ever_active[a] = ever;
-            p.sic_last[a] = factor;
-        }
-        const unsigned ballot = __ballot_sync(0xffffffffu, any_active);
-        if ((threadIdx.x & 31) == 0 && a < rc.n_astro) {
-            u32* word = w.astro_active + static_cast<u64>(buf) * w.astro_words + (a >> 5);
-            if (s_begin == 0) *word = ballot; else if (ballot) atomicOr(word, ballot);
-        }
-        return;
-    }
-    // ---------------------------------------------------------------- neurons
-    const u32 j = (blockIdx.x - astro_blocks) * blockDim.x + threadIdx.x;
-    if (j >= rc.n_neurons) return;
-    const bool excitatory = j < rc.n_exc;
-    const NeuronK& pk = excitatory ? rc.pe : rc.pi;
-    const u64 nN = rc.n_neurons;
-
-    // synaptic input of the window: deposits (push) or the row walk (pull)
-    R ex_acc[kMaxWindow], in_acc[kMaxWindow];
-    const u64 slot_base = static_cast<u64>(buf) * nN + j;
-    const u32 c = w.nin_cnt[slot_base];
-    const bool syn_input = pull || c > 0;
-    if (syn_input)
-        for (int i = 0; i < W; ++i) ex_acc[i] = in_acc[i] = static_cast<R>(0.0);
-    if (pull || c > kInboxSlots) {
-        const u32* words = w.spk_word + static_cast<u64>(prev) * nN;
-        const R* vals = w.spk_val + static_cast<u64>(prev) * W * nN;
-        pull_row<R>(p.exc_rs, p.exc_src, j, words, vals, nN, s_begin, s_end, ex_acc);
-        pull_row<R>(p.inh_rs, p.inh_src, j, words, vals, nN, s_begin, s_end, in_acc);
-    } else if (c > 0) {
-        Deposit<R> d[kInboxSlots];
-        for (u32 i = 0; i < c; ++i) d[i] = w.nin_ent[slot_base * kInboxSlots + i];
-        sort_deposits<R>(d, static_cast<int>(c));
-        for (u32 i = 0; i < c; ++i) {
-            const int st = static_cast<int>(d[i].meta & 0xFFu);
-            if (st < s_begin || st >= s_end) continue;
-            if ((d[i].meta >> 8) == 0) ex_acc[st] += d[i].val; else in_acc[st] += d[i].val;
-        }
-    }
-    if (window_done && c) w.nin_cnt[slot_base] = 0;
-
-    // SIC factors of the previous window through the active-astrocyte bitmask
-    R sic_acc[kMaxWindow];
-    bool sic_input = false;
-    {
-        const u32* act = w.astro_active + static_cast<u64>(prev) * w.astro_words;
-        const R* fac = w.sic_win + static_cast<u64>(prev) * rc.n_astro * W;
-        const u32 k1 = p.sic_rs[j + 1];
-        for (u32 k = p.sic_rs[j]; k < k1; ++k) {
-            const u32 a = p.sic_src[k];
-            if (!((act[a >> 5] >> (a & 31)) & 1u)) continue;  // every factor of this astrocyte was 0
-            if (!sic_input) {
-                for (int i = 0; i < W; ++i) sic_acc[i] = static_cast<R>(0.0);
-                sic_input = true;
-            }
-            const R* f = fac + static_cast<u64>(a) * W;
-            for (int st = s_begin; st < s_end; ++st) sic_acc[st] += f[st];
-        }
-    }
-
-    NeuronRegs<R> n{p.V[j], p.w[j], p.V_reset[j], p.b[j], p.g_ex[j], p.dg_ex[j], p.g_in[j], p.dg_in[j], p.I_sic[j],
-                    p.refr[j]};
-    const R hs = static_cast<R>(rc.h_step);
-    const R ex_decay = exp_r(-hs / static_cast<R>(pk.tau_syn_ex));
-    const R in_decay = exp_r(-hs / static_cast<R>(pk.tau_syn_in));
-    const double nstd = excitatory ? rc.noise_exc : rc.noise_inh;
-    const bool has_noise = nstd > 0.0 && rc.independent_noise;
-    u64 noise_idx_cached = ~0ull;
-    double noise = 0.0;
-    u64 pbase = step_base(rc.seed, kNeuronPoissonKey, win_start + s_begin, j);
-    u32 word = 0;
-    R* vout = w.spk_val + static_cast<u64>(buf) * W * nN;
-    for (int st = s_begin; st < s_end; ++st) {
-        const i64 t = win_start + st;
-        const bool refresh = (t - rc.d_a2n >= 0) && ((t - rc.d_a2n) % rc.sic_interval == 0);
-        if (has_noise) {
-            const u64 idx = static_cast<u64>(t / rc.steps_per_noise);
-            if (idx != noise_idx_cached) {
-                noise = neuron_noise<R>(rc, nstd, idx, j);
-                noise_idx_cached = idx;
-            }
-        }
-        const R zero = static_cast<R>(0.0);
-        const bool spiked = neuron_advance_step<R>(
-            rc, pk, excitatory, n, syn_input ? ex_acc[st] : zero, syn_input ? in_acc[st] : zero, refresh,
-            sic_input ? sic_acc[st] : zero, has_noise, noise, pbase, ex_decay, in_decay);
-        pbase += kStepAdvance;
-        if (spiked) {
-            const R out = stp_on_spike<R>(rc, p.stp_x[j], p.stp_u[j], p.stp_t[j], t);
-            vout[static_cast<u64>(st) * nN + j] = out;
-            word |= 1u << st;
-            const u32 slot = atomicAdd(&w.spk_count[buf], 1u);
-            if (slot < w.cap) w.spk_list[static_cast<u64>(buf) * w.cap + slot] = (j << 5) | static_cast<u32>(st);
-            atomicAdd(&p.counts[t], 1u);
-            if (t < p.raster_steps) atomicOr(&p.raster[static_cast<u64>(t) * rc.words + (j >> 5)], 1u << (j & 31));
-        }
-    }
-    p.V[j] = n.V;
-    p.w[j] = n.w;
-    p.g_ex[j] = n.g_ex;
-    p.dg_ex[j] = n.dg_ex;
-    p.g_in[j] = n.g_in;
-    p.dg_in[j] = n.dg_in;
-    p.I_sic[j] = n.I_sic;
-    p.refr[j] = n.refr;
-    u32* sw = w.spk_word + slot_base;
-    *sw = s_begin == 0 ? word : (*sw | word);
+    const bool astro = blockIdx.x < astro_blocks;
+    window_cells<R>(rc, p, w, win_start, s_begin, s_end, buf, mark, astro ? blockIdx.x : blockIdx.x - astro_blocks,
+                    astro);
 }
 
-// After window `buf` completes: deliver its spikes into the inboxes of the next
-// window (buffer buf ^ 1), or switch the next window to pull when it was busy.
 template <typename R>
 __global__ void push_kernel(WinPtrs<R> w, u32 n_exc, u32 n_inh, u64 n_neurons, u64 n_astro, int buf) {
-    const int nxt = buf ^ 1;
-    const u32 n = w.spk_count[buf];
-    const bool busy = n > w.push_limit;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        w.mode[nxt] = busy ? 1 : 0;
-        w.spk_count[nxt] = 0;  // the next window appends its spikes there
-    }
-    if (busy) return;
-    const u32 lane = threadIdx.x & 31;
-    const u64 warp = (static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    const u64 n_warps = (static_cast<u64>(gridDim.x) * blockDim.x) >> 5;
-    const R* vals = w.spk_val + static_cast<u64>(buf) * w.W * n_neurons;
-    for (u64 e = warp; e < n; e += n_warps) {
-        const u32 packed = w.spk_list[static_cast<u64>(buf) * w.cap + e];
-        const u32 j = packed >> 5, st = packed & 31u;
-        const R v = vals[static_cast<u64>(st) * n_neurons + j];
-        if (j < n_exc) {
-            for (u32 k = w.fe_rs[j] + lane; k < w.fe_rs[j + 1]; k += 32) {
-                const u32 t = w.fe_dst[k];
-                const u64 sb = static_cast<u64>(nxt) * n_neurons + t;
-                const u32 slot = atomicAdd(&w.nin_cnt[sb], 1u);
-                if (slot < kInboxSlots) w.nin_ent[sb * kInboxSlots + slot] = Deposit<R>{j, st, v};
-            }
-            for (u32 k = w.fa_rs[j] + lane; k < w.fa_rs[j + 1]; k += 32) {
-                const u32 a = w.fa_astro[k];
-                const u64 sb = static_cast<u64>(nxt) * n_astro + a;
-                const u32 slot = atomicAdd(&w.ain_cnt[sb], 1u);
-                if (slot < kInboxSlots) w.ain_ent[sb * kInboxSlots + slot] = Deposit<R>{w.fa_pos[k], st, v};
-            }
-        }
-        // the inhibitory rows hold local inhibitory ids and read the spike ring by
-        // global id (src/astrosim_fused.cu:458-463): neuron j feeds them when j < n_inh
-        if (j < n_inh) {
-            for (u32 k = w.fi_rs[j] + lane; k < w.fi_rs[j + 1]; k += 32) {
-                const u32 t = w.fi_dst[k];
-                const u64 sb = static_cast<u64>(nxt) * n_neurons + t;
-                const u32 slot = atomicAdd(&w.nin_cnt[sb], 1u);
-                if (slot < kInboxSlots) w.nin_ent[sb * kInboxSlots + slot] = Deposit<R>{j, st | (1u << 8), v};
-            }
-        }
-    }
+    push_cells<R>(w, n_exc, n_inh, n_neurons, n_astro, buf, blockIdx.x, gridDim.x);
 }
 
 // ------------------------------------------------------------------ forward CSRs

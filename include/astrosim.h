@@ -201,6 +201,42 @@ int astrosim_last_step_ms(astrosim_handle* h, double* ms);
  */
 int astrosim_device_info(int device, char* name, size_t name_cap, int* major, int* minor);
 
+/* ------------------------------------------------------------------ batched ensemble
+ * Many independent networks (each described by its own astrosim_config: size,
+ * seed, drive scale, weights) stepped together: one launch per 1 ms window covers
+ * every cell of every network, and the window sequence is replayed from a CUDA
+ * graph.  The reference has no batched form; it runs one network per process
+ * (src/astrosim_fused.cu:791).  Every network's results are bit-identical to
+ * running it alone through astrosim_create/astrosim_step.  All networks must share
+ * dt, substeps, precision and device.
+ */
+typedef struct astrosim_ensemble astrosim_ensemble;
+
+/* Builds every network (concurrently) and its state. */
+int astrosim_ensemble_create(const astrosim_config* cfgs, uint32_t n_networks, astrosim_ensemble** out);
+
+/* Advances every network by n_steps (a whole number of windows, 1 ms each); a
+   network stops at its own pre_ms + sim_ms. */
+int astrosim_ensemble_step(astrosim_ensemble* e, int64_t n_steps);
+
+/* Summary of network `index`, as astrosim_summary. */
+int astrosim_ensemble_summary(astrosim_ensemble* e, uint32_t index, astrosim_summary_t* out);
+
+/* State array of network `index`, as astrosim_get_state. */
+int astrosim_ensemble_get_state(astrosim_ensemble* e, uint32_t index, int which, double* dst, size_t count);
+
+/* Spike counts of network `index`, as astrosim_spike_counts. */
+int astrosim_ensemble_spike_counts(astrosim_ensemble* e, uint32_t index, int64_t first_step, int64_t n,
+                                   uint32_t* counts);
+
+/* Device time of the last astrosim_ensemble_step, ms. */
+int astrosim_ensemble_last_step_ms(astrosim_ensemble* e, double* ms);
+
+/* Wall time of astrosim_ensemble_create (all builds), seconds. */
+int astrosim_ensemble_build_seconds(astrosim_ensemble* e, double* seconds);
+
+int astrosim_ensemble_destroy(astrosim_ensemble* e);
+
 /*
  * Astrocyte summary totals over caller-provided device arrays (the layout the
  * library reduces internally for astrosim_summary).
