@@ -79,6 +79,16 @@ def lib():
                  "astrosim_ensemble_get_state", "astrosim_ensemble_spike_counts", "astrosim_ensemble_last_step_ms",
                  "astrosim_ensemble_build_seconds", "astrosim_ensemble_destroy"):
         getattr(L, name).restype = C.c_int
+    S = C.c_void_p
+    L.astrosim_server_create.argtypes = [C.c_int, C.c_int, C.c_uint64, C.c_int, C.POINTER(S)]
+    L.astrosim_server_submit.argtypes = [S, C.POINTER(abi.Config), C.POINTER(C.c_uint64)]
+    L.astrosim_server_pump.argtypes = [S, C.c_int64]
+    L.astrosim_server_result.argtypes = [S, C.c_uint64, C.POINTER(abi.RequestResult), C.POINTER(C.c_int)]
+    L.astrosim_server_get_stats.argtypes = [S, C.POINTER(abi.ServerStats)]
+    L.astrosim_server_destroy.argtypes = [S]
+    for name in ("astrosim_server_create", "astrosim_server_submit", "astrosim_server_pump", "astrosim_server_result",
+                 "astrosim_server_get_stats", "astrosim_server_destroy"):
+        getattr(L, name).restype = C.c_int
     for name in ("astrosim_create", "astrosim_step", "astrosim_summary", "astrosim_destroy",
                  "astrosim_spike_counts", "astrosim_raster", "astrosim_get_state", "astrosim_get_csr",
                  "astrosim_dump_edges", "astrosim_last_step_ms", "astrosim_device_info"):
@@ -241,6 +251,57 @@ class Ensemble:
         s = C.c_double()
         check(lib().astrosim_ensemble_build_seconds(self._h, C.byref(s)))
         return s.value
+
+
+class Server:
+    """Continuous-batching request loop (astrosim_server_*)."""
+
+    def __init__(self, precision="fp32", device=0, budget_bytes=0, builders=8):
+        prec = {"fp64": abi.PRECISION_FP64, "fp32": abi.PRECISION_FP32}[precision]
+        self.precision = precision
+        self._h = C.c_void_p()
+        check(lib().astrosim_server_create(device, prec, budget_bytes, builders, C.byref(self._h)))
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().astrosim_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, cfg=None, **overrides):
+        cfg = cfg if cfg is not None else default_config(precision=self.precision, **overrides)
+        rid = C.c_uint64()
+        check(lib().astrosim_server_submit(self._h, C.byref(cfg), C.byref(rid)))
+        return rid.value
+
+    def pump(self, windows=10):
+        check(lib().astrosim_server_pump(self._h, int(windows)))
+
+    def result(self, rid):
+        r = abi.RequestResult()
+        done = C.c_int()
+        check(lib().astrosim_server_result(self._h, rid, C.byref(r), C.byref(done)))
+        if not done.value:
+            return None
+        out = r.summary.as_dict()
+        out.update(latency_s=r.latency_s, queue_s=r.queue_s, build_s=r.build_s, run_s=r.run_s)
+        return out
+
+    def stats(self):
+        s = abi.ServerStats()
+        check(lib().astrosim_server_get_stats(self._h, C.byref(s)))
+        return s.as_dict()
 
 
 def rate_hz(spikes, n_neurons, ms):

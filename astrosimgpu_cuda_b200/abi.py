@@ -69,6 +69,20 @@ class Summary(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class RequestResult(C.Structure):
+    _fields_ = [("summary", Summary), ("latency_s", C.c_double), ("queue_s", C.c_double), ("build_s", C.c_double),
+                ("run_s", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("done", C.c_uint64), ("failed", C.c_uint64), ("pending", C.c_uint64),
+                ("building", C.c_uint64), ("running", C.c_uint64), ("bytes_in_use", C.c_uint64),
+                ("budget_bytes", C.c_uint64), ("uptime_s", C.c_double)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 def default_config(**overrides):
     """Python-side twin of astrosim_config_default (reference defaults, src/astrosim_fused.cu:792-805)."""
     cfg = Config()

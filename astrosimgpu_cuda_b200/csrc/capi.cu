@@ -13,6 +13,7 @@
 #include "../../include/astrosim.h"
 #include "ensemble.cuh"
 #include "reduce.cuh"
+#include "server.cuh"
 #include "sim.cuh"
 
 struct astrosim_handle {
@@ -21,6 +22,10 @@ struct astrosim_handle {
 
 struct astrosim_ensemble {
     astrosim::Ensemble ens;
+};
+
+struct astrosim_server {
+    astrosim::Server srv;
 };
 
 namespace {
@@ -215,6 +220,67 @@ int astrosim_ensemble_build_seconds(astrosim_ensemble* e, double* seconds) {
 
 int astrosim_ensemble_destroy(astrosim_ensemble* e) {
     delete e;
+    g_last_error.clear();
+    return ASTROSIM_OK;
+}
+
+int astrosim_server_create(int device, int precision, uint64_t hbm_budget_bytes, int builder_threads,
+                           astrosim_server** out) {
+    if (!out) return fail(ASTROSIM_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    astrosim_server* s = nullptr;
+    try {
+        s = new astrosim_server();
+    } catch (...) {
+        return fail(ASTROSIM_ERR_OUT_OF_MEMORY, "host allocation failed");
+    }
+    const int rc = guarded([&] { return s->srv.create(device, precision, hbm_budget_bytes, builder_threads); });
+    if (rc != ASTROSIM_OK) {
+        const std::string msg = g_last_error;
+        delete s;
+        g_last_error = msg;
+        return rc;
+    }
+    *out = s;
+    return ASTROSIM_OK;
+}
+
+int astrosim_server_submit(astrosim_server* s, const astrosim_config* cfg, uint64_t* request_id) {
+    if (!s || !cfg || !request_id) return fail(ASTROSIM_ERR_INVALID_ARG, "null argument");
+    if (cfg->struct_size != sizeof(astrosim_config))
+        return fail(ASTROSIM_ERR_INVALID_ARG, "astrosim_config.struct_size mismatch");
+    return guarded([&] {
+        astrosim::u64 id = 0;
+        astrosim::Status st = s->srv.submit(*cfg, &id);
+        *request_id = id;
+        return st;
+    });
+}
+
+int astrosim_server_pump(astrosim_server* s, int64_t windows) {
+    if (!s) return fail(ASTROSIM_ERR_INVALID_ARG, "null server");
+    return guarded([&] { return s->srv.pump(windows); });
+}
+
+int astrosim_server_result(astrosim_server* s, uint64_t request_id, astrosim_request_result* out, int* done) {
+    if (!s || !out || !done) return fail(ASTROSIM_ERR_INVALID_ARG, "null argument");
+    return guarded([&] {
+        bool d = false;
+        astrosim::Status st = s->srv.result(request_id, *out, &d);
+        *done = d ? 1 : 0;
+        return st;
+    });
+}
+
+int astrosim_server_get_stats(astrosim_server* s, astrosim_server_stats* out) {
+    if (!s || !out) return fail(ASTROSIM_ERR_INVALID_ARG, "null argument");
+    s->srv.stats(*out);
+    g_last_error.clear();
+    return ASTROSIM_OK;
+}
+
+int astrosim_server_destroy(astrosim_server* s) {
+    delete s;
     g_last_error.clear();
     return ASTROSIM_OK;
 }

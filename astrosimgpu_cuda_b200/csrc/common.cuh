@@ -51,19 +51,42 @@ inline Status cuda_status(cudaError_t e, const char* what, const char* file, int
         if (!_s.ok()) return _s;           \
     } while (0)
 
-// Owning device allocation (cudaMalloc / cudaFree), movable, never copied.
+// Stream for the device allocations made on this host thread (see AllocStream).
+inline cudaStream_t& alloc_stream() {
+    thread_local cudaStream_t s = nullptr;
+    return s;
+}
+
+// While alive, DevBuf allocations on this thread are stream-ordered on `s`
+// (cudaMallocAsync / cudaFreeAsync from the device's memory pool).  Plain
+// cudaFree synchronizes the whole device, which would serialize concurrent
+// network builds on different streams behind each other's kernels.
+struct AllocStream {
+    cudaStream_t prev;
+    explicit AllocStream(cudaStream_t s) : prev(alloc_stream()) { alloc_stream() = s; }
+    ~AllocStream() { alloc_stream() = prev; }
+    AllocStream(const AllocStream&) = delete;
+    AllocStream& operator=(const AllocStream&) = delete;
+};
+
+// Owning device allocation, movable, never copied.  It is freed on the stream it was
+// allocated on; the owner keeps that stream alive until its buffers are released.
 template <typename T>
 class DevBuf {
 public:
     DevBuf() = default;
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
-    DevBuf(DevBuf&& o) noexcept : p_(o.p_), n_(o.n_) { o.p_ = nullptr; o.n_ = 0; }
+    DevBuf(DevBuf&& o) noexcept : p_(o.p_), n_(o.n_), st_(o.st_) {
+        o.p_ = nullptr;
+        o.n_ = 0;
+    }
     DevBuf& operator=(DevBuf&& o) noexcept {
         if (this != &o) {
             release();
             p_ = o.p_;
             n_ = o.n_;
+            st_ = o.st_;
             o.p_ = nullptr;
             o.n_ = 0;
         }
@@ -75,10 +98,11 @@ public:
         release();
         if (n == 0) n = 1;  // keep a valid pointer for empty arrays
         void* p = nullptr;
-        cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+        st_ = alloc_stream();
+        cudaError_t e = st_ ? cudaMallocAsync(&p, n * sizeof(T), st_) : cudaMalloc(&p, n * sizeof(T));
         if (e != cudaSuccess) {
             cudaGetLastError();
-            return make_error(ASTROSIM_ERR_OUT_OF_MEMORY, "cudaMalloc of %zu bytes failed: %s", n * sizeof(T),
+            return make_error(ASTROSIM_ERR_OUT_OF_MEMORY, "device allocation of %zu bytes failed: %s", n * sizeof(T),
                               cudaGetErrorString(e));
         }
         p_ = static_cast<T*>(p);
@@ -91,7 +115,9 @@ public:
         return Status::Ok();
     }
     void release() {
-        if (p_) cudaFree(p_);
+        if (p_) {
+            if (st_) cudaFreeAsync(p_, st_); else cudaFree(p_);
+        }
         p_ = nullptr;
         n_ = 0;
     }
@@ -102,7 +128,17 @@ public:
 private:
     T* p_ = nullptr;
     size_t n_ = 0;
+    cudaStream_t st_ = nullptr;
 };
+
+// Keeps freed stream-ordered memory in the device pool (up to `bytes`) for reuse.
+inline void keep_pool_memory(int device, unsigned long long bytes) {
+    cudaMemPool_t pool = nullptr;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess && pool) {
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &bytes);
+    }
+    cudaGetLastError();
+}
 
 inline unsigned ceil_div(uint64_t a, uint64_t b) { return static_cast<unsigned>((a + b - 1) / b); }
 

@@ -101,11 +101,20 @@ Status build_descs(std::vector<std::unique_ptr<Simulation>>& nets, DevBuf<unsign
 }  // namespace
 
 Ensemble::~Ensemble() {
+    if (stream_) cudaStreamSynchronize(stream_);
     if (graph_) cudaGraphExecDestroy(graph_);
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
     nets_.clear();
-    if (stream_) cudaStreamDestroy(stream_);
+    descs_.release();
+    tile_net_.release();
+    tile_blk_.release();
+    win_.release();
+    stop_.release();
+    if (stream_) {
+        cudaStreamSynchronize(stream_);
+        cudaStreamDestroy(stream_);
+    }
 }
 
 Status Ensemble::init_empty(bool fp32, int window, int device) {
@@ -151,6 +160,7 @@ Status Ensemble::create(const astrosim_config* cfgs, u32 n) {
         if (!nets_[i]->windowed() || nets_[i]->consts().d_e != nets_[0]->consts().d_e)
             return make_error(ASTROSIM_ERR_UNSUPPORTED, "ensemble networks need the windowed engine with one window");
     AS_TRY(init_empty(cfgs[0].precision == ASTROSIM_PRECISION_FP32, nets_[0]->consts().d_e, cfgs[0].device));
+    AllocStream alloc_scope(stream_);
     win_host_.assign(n, 0);
     AS_TRY(win_.alloc_zero(n, stream_));
     std::vector<i64> stops(n);
@@ -164,6 +174,7 @@ Status Ensemble::create(const astrosim_config* cfgs, u32 n) {
 
 Status Ensemble::rebuild() {
     AS_CUDA(cudaSetDevice(device_));
+    AllocStream alloc_scope(stream_);
     if (fp32_) AS_TRY(build_descs<float>(nets_, descs_, stream_));
     else AS_TRY(build_descs<double>(nets_, descs_, stream_));
     std::vector<u32> tn, tb;
@@ -357,6 +368,7 @@ Status Ensemble::add(std::unique_ptr<Simulation> sim) {
             break;
         }
     const i64 stop = sim->total_steps();
+    AllocStream alloc_scope(stream_);
     if (slot == nets_.size()) {
         nets_.push_back(std::move(sim));
         win_host_.push_back(0);

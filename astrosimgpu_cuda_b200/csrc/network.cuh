@@ -11,12 +11,18 @@ namespace astrosim {
 
 // Target-keyed CSR (src/astrosim_fused.cu:296-301): row_start[n_targets + 1], src[n_edges].
 struct DeviceCSR {
+    DeviceCSR() = default;
+    DeviceCSR(DeviceCSR&&) = default;
+    DeviceCSR& operator=(DeviceCSR&&) = default;
     DevBuf<u32> row_start, src;
     u32 n_targets = 0;
     u64 n_edges = 0;
 };
 
 struct Network {
+    Network() = default;
+    Network(Network&&) = default;
+    Network& operator=(Network&&) = default;
     Sizes sz;
     u64 seed = 0;
     DeviceCSR exc, inh, sic, e2a;
@@ -30,7 +36,7 @@ struct BuildOptions {
     // Networks whose estimated connectivity stream is shorter than this many draws are
     // walked by one device thread (exact, no setup overhead); larger ones by the chunked
     // parallel builder.  0 forces the parallel builder, UINT64_MAX the sequential one.
-    u64 sequential_max_draws = 4000000ULL;
+    u64 sequential_max_draws = 50000ULL;
 };
 
 // Builds connectivity and per-cell parameters for (sizes, seed, biology) on `stream`,

@@ -95,10 +95,18 @@ Biology biology_for(const astrosim_config& cfg) {
 }  // namespace
 
 Simulation::~Simulation() {
+    // buffers are freed on stream_ (stream-ordered), so release them before the stream goes
+    if (stream_) cudaStreamSynchronize(stream_);
     delete win_;
+    win_ = nullptr;
+    st_ = StateBuffers();
+    net_ = Network();
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
-    if (stream_) cudaStreamDestroy(stream_);
+    if (stream_) {
+        cudaStreamSynchronize(stream_);
+        cudaStreamDestroy(stream_);
+    }
 }
 
 Status Simulation::create(const astrosim_config& cfg) {
@@ -127,6 +135,8 @@ Status Simulation::create(const astrosim_config& cfg) {
     AS_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     AS_CUDA(cudaEventCreate(&ev0_));
     AS_CUDA(cudaEventCreate(&ev1_));
+    keep_pool_memory(device_, 8ull << 30);
+    AllocStream alloc_scope(stream_);
 
     bio_ = biology_for(cfg);
     const Sizes sz = scaling_law(cfg.n_total);
@@ -240,6 +250,7 @@ Status Simulation::create(const astrosim_config& cfg) {
 
 Status Simulation::ensure_counts(i64 steps) {
     if (steps <= counts_cap_) return Status::Ok();
+    AllocStream alloc_scope(stream_);
     i64 cap = std::max<i64>(steps, counts_cap_ * 2);
     DevBuf<u32> nb;
     AS_TRY(nb.alloc_zero(static_cast<size_t>(cap), stream_));
@@ -417,6 +428,7 @@ Status Simulation::get_state(int which, double* dst, size_t count) {
     if (dptr) {
         AS_CUDA(cudaMemcpyAsync(dst, dptr, n * sizeof(double), cudaMemcpyDeviceToHost, stream_));
     } else {
+        AllocStream alloc_scope(stream_);
         DevBuf<double> tmp;
         AS_TRY(tmp.alloc(n));
         if (fp32_)

@@ -36,6 +36,9 @@ struct RunConsts {
 // Device state arrays.  V, w, Ca and IP3 are double in every precision; the
 // remaining state and the rings are `real` (double or float).
 struct StateBuffers {
+    StateBuffers() = default;
+    StateBuffers(StateBuffers&&) = default;
+    StateBuffers& operator=(StateBuffers&&) = default;
     DevBuf<double> V, w, Ca, IP3;
     DevBuf<unsigned char> g_raw;  // g_ex, dg_ex, g_in, dg_in, I_sic, h, stp_x, stp_u as `real` (8 arrays)
     DevBuf<double> stp_t;

@@ -285,6 +285,131 @@ def run_reference(args, ws, rank):
     }
 
 
+def reference_sequential(cfgs, sample):
+    """Wall time per network of the reference program run once per network (its FP32 build)."""
+    binary = os.path.join(REPO, "oracle", "_ref", "astrosim_fused_ref_f32")
+    if not os.path.exists(binary):
+        return None
+    times = []
+    for i in sample:
+        c = cfgs[i]
+        cmd = [binary, "--n", str(c.n_total), "--seed", str(c.seed), "--pre-ms", f"{c.pre_ms:g}",
+               "--sim-ms", f"{c.sim_ms:g}", "--w-a2n", f"{c.w_a2n:g}"]
+        t = time.perf_counter()
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+        if r.returncode != 0:
+            return None
+        times.append(time.perf_counter() - t)
+    return sum(times) / len(times)
+
+
+def ours_sequential(cfgs, sample):
+    import astrosimgpu_cuda_b200 as asg
+    times = []
+    for i in sample:
+        t = time.perf_counter()
+        with asg.Simulation(cfgs[i]) as sim:
+            sim.step(sim.summary()["total_steps"])
+            sim.summary()
+        times.append(time.perf_counter() - t)
+    return sum(times) / len(times)
+
+
+def run_ensemble(args):
+    """256 networks, N_total log-uniform in [500, 50000], 2000 ms each, FP32 (the batched configuration)."""
+    import numpy as np
+
+    import astrosimgpu_cuda_b200 as asg
+    from astrosimgpu_cuda_b200 import abi
+
+    rng = np.random.default_rng(2026)
+    n = args.ens_networks
+    cfgs = [abi.default_config(n_total=int(np.exp(rng.uniform(np.log(500), np.log(50000)))), seed=1000 + i,
+                               pre_ms=0.0, sim_ms=2000.0, precision="fp32",
+                               neuron_drive_scale=float(rng.uniform(0.8, 1.2)), w_a2n=float(rng.uniform(0.8, 1.2)))
+            for i in range(n)]
+    t0 = time.perf_counter()
+    with asg.Ensemble(cfgs) as ens:
+        build_s = ens.build_seconds()
+        ens.step(20000)
+        step_ms = ens.last_step_ms()
+        rates = [ens.summary(i)["mean_rate_hz"] for i in range(n)]
+    wall = time.perf_counter() - t0
+    sample = [int(x) for x in rng.choice(n, size=min(n, args.baseline_sample), replace=False)]
+    ours = ours_sequential(cfgs, sample)
+    ref = reference_sequential(cfgs, sample)
+    out = {"networks": n, "n_total_sum": int(sum(c.n_total for c in cfgs)), "sim_ms": 2000.0, "dtype": "f32",
+           "sims_per_s": n / wall, "sims_per_s_stepping_only": n / (step_ms * 1e-3),
+           "build_s": build_s, "stepping_s": step_ms * 1e-3, "wall_s": wall,
+           "mean_rate_hz": float(np.mean(rates)),
+           "plain_path_sequential_sims_per_s": 1.0 / ours,
+           "baseline_sample": f"{len(sample)} of the {n} networks, run one after another",
+           "speedup_vs_plain_path_sequential": (n / wall) * ours}
+    if ref:
+        out["reference_sequential_sims_per_s"] = 1.0 / ref
+        out["speedup_vs_reference_sequential"] = (n / wall) * ref
+        out["reference_note"] = "unmodified reference FP32 build, one process per network (its host build, " \
+                                "default drive rate: it has no drive flag)"
+    return out
+
+
+def run_serving(args, rate):
+    """Open-loop Poisson arrivals of simulation requests (N log-uniform in [1e3, 2e5], 200-2000 ms)."""
+    import numpy as np
+
+    import astrosimgpu_cuda_b200 as asg
+    from astrosimgpu_cuda_b200 import abi
+
+    rng = np.random.default_rng(7 + int(rate))
+    n = args.serve_requests
+    cfgs = [abi.default_config(n_total=int(np.exp(rng.uniform(np.log(1e3), np.log(2e5)))),
+                               seed=int(rng.integers(1, 1 << 40)), pre_ms=0.0,
+                               sim_ms=float(int(rng.uniform(200, 2000))), precision="fp32",
+                               neuron_drive_scale=float(rng.uniform(0.8, 1.2))) for _ in range(n)]
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n))
+    submit_t = np.zeros(n)
+    ids = []
+    deadline = args.serve_timeout
+    with asg.Server(precision="fp32", builders=16) as srv:
+        t0 = time.perf_counter()
+        i = 0
+        while True:
+            now = time.perf_counter() - t0
+            while i < n and arrivals[i] <= now:
+                ids.append(srv.submit(cfgs[i]))
+                submit_t[i] = time.perf_counter() - t0
+                i += 1
+            st = srv.stats()
+            if i == n and st["done"] == n:
+                break
+            if now > deadline:
+                break
+            if st["running"] == 0 and st["building"] == 0 and st["pending"] == 0 and i < n:
+                time.sleep(max(0.0, min(0.01, arrivals[i] - now)))
+                continue
+            srv.pump(args.serve_pump_windows)
+            if st["running"] == 0:
+                time.sleep(0.0005)
+        res = [srv.result(r) for r in ids]
+        stats = srv.stats()
+    done = [(k, r) for k, r in enumerate(res) if r is not None]
+    lat = np.array([r["latency_s"] for _, r in done]) if done else np.array([np.nan])
+    finish = max(submit_t[k] + r["latency_s"] for k, r in done) if done else float("nan")
+    sample = [int(x) for x in rng.choice(n, size=min(n, args.baseline_sample), replace=False)]
+    out = {"requests": n, "completed": len(done), "arrival_rate_per_s": rate, "dtype": "f32",
+           "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
+           "mean_queue_s": float(np.mean([r["queue_s"] for _, r in done])) if done else None,
+           "sims_per_s": len(done) / finish if done else 0.0, "makespan_s": finish,
+           "budget_bytes": stats["budget_bytes"]}
+    ref = reference_sequential(cfgs, sample)
+    if ref:
+        out["reference_sequential_sims_per_s"] = 1.0 / ref
+        out["speedup_vs_reference_sequential"] = out["sims_per_s"] * ref
+    ours = ours_sequential(cfgs, sample)
+    out["plain_path_sequential_sims_per_s"] = 1.0 / ours
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -295,6 +420,14 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the whole-job run (profiling captures)")
     ap.add_argument("--n", type=int, default=N_TOTAL, help="network size (the benchmark is N=1e7)")
+    ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--ens-networks", type=int, default=256)
+    ap.add_argument("--serve-requests", type=int, default=2000)
+    ap.add_argument("--serve-rates", default="200", help="comma-separated arrival rates (req/s)")
+    ap.add_argument("--serve-pump-windows", type=int, default=10)
+    ap.add_argument("--serve-timeout", type=float, default=240.0)
+    ap.add_argument("--baseline-sample", type=int, default=8)
     args = ap.parse_args()
     globals()["N_TOTAL"] = args.n
     args.warmup = max(3, args.warmup)
@@ -342,6 +475,10 @@ def main():
         "clocks": f32["clocks"],
         "summary_fp32": extra["summary_fp32"],
     }
+    if not args.no_ensemble and ws == 1 and args.n == 10_000_000:
+        line["ensemble"] = run_ensemble(args)
+    if not args.no_serving and ws == 1 and args.n == 10_000_000:
+        line["serving"] = [run_serving(args, float(r)) for r in args.serve_rates.split(",")]
     if not args.no_cpu_baseline and ws == 1:
         try:
             line["cpu_baseline"] = cpu_baseline(args)

@@ -237,6 +237,43 @@ int astrosim_ensemble_build_seconds(astrosim_ensemble* e, double* seconds);
 
 int astrosim_ensemble_destroy(astrosim_ensemble* e);
 
+/* ------------------------------------------------------------------ serving
+ * A request loop with continuous batching (no counterpart in the reference, which
+ * runs one network per process).  Requests queue FIFO and are admitted when their
+ * estimated device footprint fits the HBM budget; their networks are built on
+ * builder threads (own CUDA streams, overlapping the running batch), join the
+ * running ensemble between windows, and leave it when they reach their last step.
+ * Each result is bit-identical to running the same configuration alone.
+ */
+typedef struct astrosim_server astrosim_server;
+
+typedef struct astrosim_request_result {
+    astrosim_summary_t summary;
+    double latency_s;  /* submit -> result ready */
+    double queue_s;    /* submit -> admitted (its footprint fit the budget) */
+    double build_s;    /* device build of its network */
+    double run_s;      /* joined the batch -> last step done */
+} astrosim_request_result;
+
+typedef struct astrosim_server_stats {
+    uint64_t submitted, done, failed, pending, building, running;
+    uint64_t bytes_in_use, budget_bytes;
+    double uptime_s;
+} astrosim_server_stats;
+
+/* hbm_budget_bytes = 0 uses 85 % of the device's free memory.  Requests must use
+   dt = 0.1 ms and the server's precision. */
+int astrosim_server_create(int device, int precision, uint64_t hbm_budget_bytes, int builder_threads,
+                           astrosim_server** out);
+int astrosim_server_submit(astrosim_server* s, const astrosim_config* cfg, uint64_t* request_id);
+/* Admits what fits, joins built networks, advances the batch by `windows` windows
+   (1 ms each) and retires finished requests. */
+int astrosim_server_pump(astrosim_server* s, int64_t windows);
+/* *done = 0 while the request is still queued or running. */
+int astrosim_server_result(astrosim_server* s, uint64_t request_id, astrosim_request_result* out, int* done);
+int astrosim_server_get_stats(astrosim_server* s, astrosim_server_stats* out);
+int astrosim_server_destroy(astrosim_server* s);
+
 /*
  * Astrocyte summary totals over caller-provided device arrays (the layout the
  * library reduces internally for astrosim_summary).
