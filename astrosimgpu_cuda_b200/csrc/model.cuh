@@ -163,6 +163,8 @@ struct AstroK {
     double SIC_scale, SIC_th;
     // Folded constants of the FP32 form (its stages multiply by reciprocals).
     float f_inv_ratio, f_ratio_rate_IP3R, f_ratio_rate_L, f_k_Kd_inh, f_Km2;
+    // Float copies read by the FP32 stages (converted once here, not per use).
+    float f_Kd_IP3_1, f_Kd_IP3_2, f_Kd_act, f_rate_SERCA, f_k_IP3R, f_SIC_scale;
 };
 
 // AdEx neuron constants for one population (src/astrosim_fused.cu:228-232).
@@ -175,6 +177,11 @@ struct NeuronK {
     double inv_Delta_T_pow2;
     // Folded constants of the FP32 form.
     float f_gL_DT, f_inv_DT, f_inv_Cm, f_inv_tauw;
+    // Float copies read by the FP32 stages (converted once here, not per use).
+    float f_V_peak, f_E_L, f_V_th, f_E_ex, f_E_in, f_g_L, f_I_e, f_a, f_psc_init_ex, f_psc_init_in;
+    // Refractory length in steps, static_cast<int>(t_ref / h_step + 0.5) (src/astrosim_fused.cu:555);
+    // set with the step size.
+    int ref_steps;
 };
 
 // Biology defaults, compiled into the reference (src/astrosim_fused.cu:742-781).
@@ -222,6 +229,12 @@ inline AstroK astro_constants(const Biology& b) {  // src/astrosim_fused.cu:935-
     k.f_ratio_rate_L = static_cast<float>(b.ratio_ER_cyt * b.rate_L);
     k.f_k_Kd_inh = static_cast<float>(b.k_IP3R * b.Kd_inh);
     k.f_Km2 = static_cast<float>(b.Km_SERCA * b.Km_SERCA);
+    k.f_Kd_IP3_1 = static_cast<float>(b.Kd_IP3_1);
+    k.f_Kd_IP3_2 = static_cast<float>(b.Kd_IP3_2);
+    k.f_Kd_act = static_cast<float>(b.Kd_act);
+    k.f_rate_SERCA = static_cast<float>(b.rate_SERCA);
+    k.f_k_IP3R = static_cast<float>(b.k_IP3R);
+    k.f_SIC_scale = static_cast<float>(b.SIC_scale);
     return k;
 }
 
@@ -250,6 +263,17 @@ inline NeuronK neuron_constants(const Biology& b, bool exc) {  // src/astrosim_f
     k.f_inv_DT = static_cast<float>(1.0 / k.Delta_T);
     k.f_inv_Cm = static_cast<float>(1.0 / k.C_m);
     k.f_inv_tauw = static_cast<float>(1.0 / k.tau_w);
+    k.f_V_peak = static_cast<float>(k.V_peak);
+    k.f_E_L = static_cast<float>(k.E_L);
+    k.f_V_th = static_cast<float>(k.V_th);
+    k.f_E_ex = static_cast<float>(k.E_ex);
+    k.f_E_in = static_cast<float>(k.E_in);
+    k.f_g_L = static_cast<float>(k.g_L);
+    k.f_I_e = static_cast<float>(k.I_e);
+    k.f_a = static_cast<float>(k.a);
+    k.f_psc_init_ex = static_cast<float>(k.psc_init_ex);
+    k.f_psc_init_in = static_cast<float>(k.psc_init_in);
+    k.ref_steps = 0;
     return k;
 }
 
@@ -301,14 +325,12 @@ __device__ __forceinline__ void neuron_rhs(const NeuronK& p, double V, double w,
 // hardware exponential (stage arithmetic only; V and w accumulate in double).
 __device__ __forceinline__ void neuron_rhs(const NeuronK& p, float V, float w, float g_ex, float g_in, float I_ext,
                                            float& dV, float& dw) {
-    const float V_peak = static_cast<float>(p.V_peak), E_L = static_cast<float>(p.E_L);
-    const float Vc = V < V_peak ? V : V_peak;
-    const float I_spike = p.f_gL_DT * __expf((Vc - static_cast<float>(p.V_th)) * p.f_inv_DT);
-    const float I_syn_ex = g_ex * (Vc - static_cast<float>(p.E_ex));
-    const float I_syn_in = g_in * (Vc - static_cast<float>(p.E_in));
-    dV = (-static_cast<float>(p.g_L) * (Vc - E_L) + I_spike - I_syn_ex - I_syn_in - w + static_cast<float>(p.I_e) +
-          I_ext) * p.f_inv_Cm;
-    dw = (static_cast<float>(p.a) * (Vc - E_L) - w) * p.f_inv_tauw;
+    const float Vc = V < p.f_V_peak ? V : p.f_V_peak;
+    const float I_spike = p.f_gL_DT * __expf((Vc - p.f_V_th) * p.f_inv_DT);
+    const float I_syn_ex = g_ex * (Vc - p.f_E_ex);
+    const float I_syn_in = g_in * (Vc - p.f_E_in);
+    dV = (-p.f_g_L * (Vc - p.f_E_L) + I_spike - I_syn_ex - I_syn_in - w + p.f_I_e + I_ext) * p.f_inv_Cm;
+    dw = (p.f_a * (Vc - p.f_E_L) - w) * p.f_inv_tauw;
 }
 
 // The FP32 form of the Li-Rinzel right-hand side (see astro_rhs).
@@ -316,21 +338,28 @@ __device__ __forceinline__ void astro_rhs_fast(const AstroK& c, float Ca_tot, fl
                                                float Ca, float IP3, float h, float noise, float& dCa, float& dIP3,
                                                float& dh) {
     const float Ca_ER = (Ca_tot - Ca) * c.f_inv_ratio;
-    const float m_inf = __fdividef(IP3, IP3 + static_cast<float>(c.Kd_IP3_1));
-    const float n_inf = __fdividef(Ca, Ca + static_cast<float>(c.Kd_act));
+    const float m_inf = __fdividef(IP3, IP3 + c.f_Kd_IP3_1);
+    const float n_inf = __fdividef(Ca, Ca + c.f_Kd_act);
     const float m3 = m_inf * m_inf * m_inf;
     const float n3 = n_inf * n_inf * n_inf;
     const float h3 = h * h * h;
     const float J_channel = c.f_ratio_rate_IP3R * m3 * n3 * h3 * (Ca_ER - Ca);
-    const float J_pump = __fdividef(static_cast<float>(c.rate_SERCA) * Ca * Ca, c.f_Km2 + Ca * Ca);
+    const float J_pump = __fdividef(c.f_rate_SERCA * Ca * Ca, c.f_Km2 + Ca * Ca);
     const float J_leak = c.f_ratio_rate_L * (Ca_ER - Ca);
-    const float alpha_h = __fdividef(c.f_k_Kd_inh * (IP3 + static_cast<float>(c.Kd_IP3_1)),
-                                     IP3 + static_cast<float>(c.Kd_IP3_2));
-    const float beta_h = static_cast<float>(c.k_IP3R) * Ca;
+    const float alpha_h = __fdividef(c.f_k_Kd_inh * (IP3 + c.f_Kd_IP3_1), IP3 + c.f_Kd_IP3_2);
+    const float beta_h = c.f_k_IP3R * Ca;
     dCa = J_channel - J_pump + J_leak + noise;
     dIP3 = (IP3_0 - IP3) * inv_tau_IP3;
     dh = alpha_h * (1.0f - h) - beta_h * h;
 }
+
+// A run constant in the stage type: the double value, or its float copy.
+template <typename R>
+__host__ __device__ __forceinline__ R as_r(double d, float f);
+template <>
+__host__ __device__ __forceinline__ double as_r<double>(double d, float) { return d; }
+template <>
+__host__ __device__ __forceinline__ float as_r<float>(double, float f) { return f; }
 
 // Box-Muller in float from one stream (counters 0 and 1): the noise draws of the FP32 form.
 __device__ __forceinline__ float normal_fast(u64 base) {

@@ -30,7 +30,6 @@ namespace {
 
 constexpr int kMaxTypes = 4;
 constexpr u32 kChunkNormals = 2048;  // normals per chunk (even)
-constexpr int kMaxTries = 1000;      // src/astrosim_fused.cu:196
 
 struct TypeSpec {
     double mean, sd, lo, hi;

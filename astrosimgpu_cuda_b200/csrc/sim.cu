@@ -94,6 +94,22 @@ Biology biology_for(const astrosim_config& cfg) {
 
 }  // namespace
 
+void fill_stage_constants(RunConsts& rc) {
+    rc.h6 = rc.h_step / 6.0;
+    rc.f_h_step = static_cast<float>(rc.h_step);
+    rc.f_h6 = rc.f_h_step / 6.0f;
+    rc.f_w_e = static_cast<float>(rc.w_e);
+    rc.f_neg_w_i = static_cast<float>(-rc.w_i);
+    rc.f_w_n2a = static_cast<float>(rc.w_n2a);
+    rc.f_w_a2n = static_cast<float>(rc.w_a2n);
+    rc.f_weight_astro = static_cast<float>(rc.weight_astro);
+    rc.f_weight_exc = static_cast<float>(rc.weight_exc);
+    rc.f_weight_inh = static_cast<float>(rc.weight_inh);
+    rc.f_noise_astro = static_cast<float>(rc.noise_astro);
+    rc.pe.ref_steps = static_cast<int>(rc.pe.t_ref / rc.h_step + 0.5);
+    rc.pi.ref_steps = static_cast<int>(rc.pi.t_ref / rc.h_step + 0.5);
+}
+
 Simulation::~Simulation() {
     // buffers are freed on stream_ (stream-ordered), so release them before the stream goes
     if (stream_) cudaStreamSynchronize(stream_);
@@ -181,6 +197,7 @@ Status Simulation::create(const astrosim_config& cfg) {
     rc.n_neurons = sz.n_neurons;
     rc.n_astro = sz.n_astro;
     rc.words = (sz.n_neurons + 31) / 32;
+    fill_stage_constants(rc);
     {
         DevBuf<double> lim;
         AS_TRY(lim.alloc(3));

@@ -31,7 +31,17 @@ struct RunConsts {
     double SIC_th;
     u64 seed;
     u32 n_exc, n_neurons, n_astro, words;  // words = ceil(n_neurons / 32)
+    // Stage-type copies, converted once on the host (see fill_stage_constants):
+    // h_step / 6 for the RK4 weights, and float copies of the weights and noise.
+    double h6;
+    float f_h_step, f_h6, f_w_e, f_neg_w_i, f_w_n2a, f_w_a2n;
+    float f_weight_astro, f_weight_exc, f_weight_inh, f_noise_astro;
 };
+
+// Derives the stage-type copies in `rc` from its double fields.  Every value equals
+// what the device would compute from the double (host and device division and
+// double-to-float conversion are both IEEE round-to-nearest).
+void fill_stage_constants(RunConsts& rc);
 
 // Device state arrays.  V, w, Ca and IP3 are double in every precision; the
 // remaining state and the rings are `real` (double or float).

@@ -55,54 +55,73 @@ __device__ __forceinline__ void astro_stage(const AstroK& c, R Ct, R I0, R tI, R
     }
 }
 
-template <typename R>
-__device__ __forceinline__ void astro_advance(const AstroK& c, double Ca_tot, double IP3_0, double tau_IP3,
-                                              double delta_IP3, R ip3_input, R noise, double h_step, int substeps,
-                                              double& Ca, double& IP3, R& h) {
-    if (ip3_input != static_cast<R>(0.0)) IP3 += delta_IP3 * static_cast<double>(ip3_input);
-    const R hs = static_cast<R>(h_step);
-    const R Ct = static_cast<R>(Ca_tot), I0 = static_cast<R>(IP3_0), tI = static_cast<R>(tau_IP3);
-    const R inv_tI = static_cast<R>(1.0) / tI;  // used by the FP32 form only
-    for (int s = 0; s < substeps; ++s) {
-        const R ca = static_cast<R>(Ca), ip = static_cast<R>(IP3);
-        R k1c, k1i, k1h, k2c, k2i, k2h, k3c, k3i, k3h, k4c, k4i, k4h;
-        astro_stage<R>(c, Ct, I0, tI, inv_tI, ca, ip, h, noise, k1c, k1i, k1h);
-        astro_stage<R>(c, Ct, I0, tI, inv_tI, ca + static_cast<R>(0.5) * hs * k1c, ip + static_cast<R>(0.5) * hs * k1i,
-                       h + static_cast<R>(0.5) * hs * k1h, noise, k2c, k2i, k2h);
-        astro_stage<R>(c, Ct, I0, tI, inv_tI, ca + static_cast<R>(0.5) * hs * k2c, ip + static_cast<R>(0.5) * hs * k2i,
-                       h + static_cast<R>(0.5) * hs * k2h, noise, k3c, k3i, k3h);
-        astro_stage<R>(c, Ct, I0, tI, inv_tI, ca + hs * k3c, ip + hs * k3i, h + hs * k3h, noise, k4c, k4i, k4h);
-        Ca += static_cast<double>((hs / static_cast<R>(6.0)) *
-                                  (k1c + static_cast<R>(2.0) * k2c + static_cast<R>(2.0) * k3c + k4c));
-        IP3 += static_cast<double>((hs / static_cast<R>(6.0)) *
-                                   (k1i + static_cast<R>(2.0) * k2i + static_cast<R>(2.0) * k3i + k4i));
-        h += (hs / static_cast<R>(6.0)) * (k1h + static_cast<R>(2.0) * k2h + static_cast<R>(2.0) * k3h + k4h);
-        Ca = Ca < 0.0 ? 0.0 : (Ca > Ca_tot ? Ca_tot : Ca);
-        h = h < static_cast<R>(0.0) ? static_cast<R>(0.0) : (h > static_cast<R>(1.0) ? static_cast<R>(1.0) : h);
-        IP3 = IP3 < 0.0 ? 0.0 : IP3;
-    }
-}
-
 __device__ __forceinline__ double log_r(double x) { return log(x); }
 __device__ __forceinline__ float log_r(float x) { return logf(x); }
 
-// Register-resident state of one astrocyte.
+// Register-resident state of one astrocyte.  The parameters are kept in double
+// (the accumulator updates and clamps use them) and in the stage type, converted
+// once per load rather than once per step.
 template <typename R>
 struct AstroRegs {
     double Ca, IP3;
     R h;
     double Ca_tot, IP3_0, tau_IP3, delta_IP3;
+    R Ct, I0, tI, inv_tI;  // stage copies of Ca_tot, IP3_0, tau_IP3 and 1 / tau_IP3 (FP32 form only)
 };
+
+template <typename R>
+__device__ __forceinline__ AstroRegs<R> load_astro(double Ca, double IP3, R h, double Ca_tot, double IP3_0,
+                                                   double tau_IP3, double delta_IP3) {
+    AstroRegs<R> s;
+    s.Ca = Ca;
+    s.IP3 = IP3;
+    s.h = h;
+    s.Ca_tot = Ca_tot;
+    s.IP3_0 = IP3_0;
+    s.tau_IP3 = tau_IP3;
+    s.delta_IP3 = delta_IP3;
+    s.Ct = static_cast<R>(Ca_tot);
+    s.I0 = static_cast<R>(IP3_0);
+    s.tI = static_cast<R>(tau_IP3);
+    s.inv_tI = static_cast<R>(1.0) / s.tI;  // used by the FP32 form only
+    return s;
+}
+
+// One step of the astrocyte ODEs: the IP3 kick, then Li-Rinzel RK4 with clamps
+// (src/astrosim_fused.cu:255-278); noise held over the stages.  hs is the substep,
+// h6 = hs / 6.
+template <typename R>
+__device__ __forceinline__ void astro_advance(const AstroK& c, AstroRegs<R>& s, R ip3_input, R noise, R hs, R h6,
+                                              int substeps) {
+    if (ip3_input != static_cast<R>(0.0)) s.IP3 += s.delta_IP3 * static_cast<double>(ip3_input);
+    for (int k = 0; k < substeps; ++k) {
+        const R ca = static_cast<R>(s.Ca), ip = static_cast<R>(s.IP3), h = s.h;
+        R k1c, k1i, k1h, k2c, k2i, k2h, k3c, k3i, k3h, k4c, k4i, k4h;
+        astro_stage<R>(c, s.Ct, s.I0, s.tI, s.inv_tI, ca, ip, h, noise, k1c, k1i, k1h);
+        astro_stage<R>(c, s.Ct, s.I0, s.tI, s.inv_tI, ca + static_cast<R>(0.5) * hs * k1c,
+                       ip + static_cast<R>(0.5) * hs * k1i, h + static_cast<R>(0.5) * hs * k1h, noise, k2c, k2i, k2h);
+        astro_stage<R>(c, s.Ct, s.I0, s.tI, s.inv_tI, ca + static_cast<R>(0.5) * hs * k2c,
+                       ip + static_cast<R>(0.5) * hs * k2i, h + static_cast<R>(0.5) * hs * k2h, noise, k3c, k3i, k3h);
+        astro_stage<R>(c, s.Ct, s.I0, s.tI, s.inv_tI, ca + hs * k3c, ip + hs * k3i, h + hs * k3h, noise, k4c, k4i,
+                       k4h);
+        s.Ca += static_cast<double>(h6 * (k1c + static_cast<R>(2.0) * k2c + static_cast<R>(2.0) * k3c + k4c));
+        s.IP3 += static_cast<double>(h6 * (k1i + static_cast<R>(2.0) * k2i + static_cast<R>(2.0) * k3i + k4i));
+        R hn = h + h6 * (k1h + static_cast<R>(2.0) * k2h + static_cast<R>(2.0) * k3h + k4h);
+        s.Ca = s.Ca < 0.0 ? 0.0 : (s.Ca > s.Ca_tot ? s.Ca_tot : s.Ca);
+        s.h = hn < static_cast<R>(0.0) ? static_cast<R>(0.0) : (hn > static_cast<R>(1.0) ? static_cast<R>(1.0) : hn);
+        s.IP3 = s.IP3 < 0.0 ? 0.0 : s.IP3;
+    }
+}
 
 // Everything astrocyte `a` does in step `step` once its delayed spike sum is known
 // (src/astrosim_fused.cu:390-417): Poisson IP3 drive, noise, RK4, SIC factor.
 template <typename R>
 __device__ __forceinline__ R astro_advance_step(const RunConsts& rc, AstroRegs<R>& s, R gathered, u32 a, i64 step,
                                                 u64 poisson_base, u64 noise_base) {
-    R ip3_input = static_cast<R>(rc.w_n2a) * gathered;
+    R ip3_input = as_r<R>(rc.w_n2a, rc.f_w_n2a) * gathered;
     if (rc.lambda_astro > 0.0) {
         const int ev = rng_poisson_at(poisson_base, rc.lambda_astro, rc.limit_astro, rc.lim53_astro);
-        if (ev > 0) ip3_input += static_cast<R>(rc.weight_astro) * static_cast<R>(ev);
+        if (ev > 0) ip3_input += as_r<R>(rc.weight_astro, rc.f_weight_astro) * static_cast<R>(ev);
     }
     R noise = static_cast<R>(0.0);
     if (rc.noise_astro > 0.0) {
@@ -110,7 +129,7 @@ __device__ __forceinline__ R astro_advance_step(const RunConsts& rc, AstroRegs<R
         if (!rc.independent_noise)
             base = rng_base(rc.seed ^ kAstroNoiseKey, static_cast<u64>(step / rc.steps_per_noise));
         if constexpr (std::is_same<R, float>::value) {
-            noise = static_cast<float>(rc.noise_astro) * normal_fast(base);
+            noise = rc.f_noise_astro * normal_fast(base);
         } else {
             double u1 = rng_uniform_at(base, 0);  // rng_normal (src/astrosim_fused.cu:143-149)
             if (u1 <= 1e-300) u1 = 1e-300;
@@ -118,12 +137,12 @@ __device__ __forceinline__ R astro_advance_step(const RunConsts& rc, AstroRegs<R
             noise = rc.noise_astro * (sqrt(-2.0 * log(u1)) * cos(kTwoPi * u2));
         }
     }
-    astro_advance<R>(rc.ak, s.Ca_tot, s.IP3_0, s.tau_IP3, s.delta_IP3, ip3_input, noise, rc.h_step, rc.substeps,
-                     s.Ca, s.IP3, s.h);
+    astro_advance<R>(rc.ak, s, ip3_input, noise, as_r<R>(rc.h_step, rc.f_h_step), as_r<R>(rc.h6, rc.f_h6),
+                     rc.substeps);
     // SIC factor (416-417); the threshold test runs on the double Ca in every precision
     const double y = (s.Ca - rc.ak.SIC_th) * 1000.0;
     R factor = static_cast<R>(0.0);
-    if (!(y <= 1.0)) factor = static_cast<R>(rc.ak.SIC_scale) * log_r(static_cast<R>(y));
+    if (!(y <= 1.0)) factor = as_r<R>(rc.ak.SIC_scale, rc.ak.f_SIC_scale) * log_r(static_cast<R>(y));
     return factor;
 }
 
@@ -141,7 +160,7 @@ __device__ __forceinline__ void astro_cell_step(const RunConsts& rc, const StepP
     const int read_slot = static_cast<int>((step + S - rc.d_e) % S);  // the e2a delay is d_e (384)
     const R gathered = gather_spikes<R>(p.e2a_rs, p.e2a_src, a, p.bits + static_cast<u64>(read_slot) * rc.words,
                                         p.val + static_cast<u64>(read_slot) * rc.n_neurons);
-    AstroRegs<R> s{p.Ca[a], p.IP3[a], p.h[a], p.Ca_tot[a], p.IP3_0[a], p.tau_IP3[a], p.delta_IP3[a]};
+    AstroRegs<R> s = load_astro<R>(p.Ca[a], p.IP3[a], p.h[a], p.Ca_tot[a], p.IP3_0[a], p.tau_IP3[a], p.delta_IP3[a]);
     const R factor = astro_advance_step<R>(rc, s, gathered, a, step, step_base(rc.seed, kAstroPoissonKey, step, a),
                                            step_base(rc.seed, kAstroNoiseKey, step, a));
     p.Ca[a] = s.Ca;
@@ -169,24 +188,27 @@ __device__ __forceinline__ bool neuron_advance_step(const RunConsts& rc, const N
                                                     NeuronRegs<R>& n, R exc_sum, R inh_sum, bool sic_refresh,
                                                     R sic_sum, bool has_noise, double noise, u64 poisson_base,
                                                     R ex_decay, R in_decay) {
-    R exc_input = static_cast<R>(rc.w_e) * exc_sum;
-    const R inh_input = static_cast<R>(-rc.w_i) * inh_sum;
+    R exc_input = as_r<R>(rc.w_e, rc.f_w_e) * exc_sum;
+    const R inh_input = as_r<R>(-rc.w_i, rc.f_neg_w_i) * inh_sum;
     const double lambda = excitatory ? rc.lambda_exc : rc.lambda_inh;
     if (lambda > 0.0) {
         const int ev = rng_poisson_at(poisson_base, lambda, excitatory ? rc.limit_exc : rc.limit_inh,
                                       excitatory ? rc.lim53_exc : rc.lim53_inh);
-        if (ev > 0) exc_input += static_cast<R>(excitatory ? rc.weight_exc : rc.weight_inh) * static_cast<R>(ev);
+        if (ev > 0)
+            exc_input += (excitatory ? as_r<R>(rc.weight_exc, rc.f_weight_exc) : as_r<R>(rc.weight_inh, rc.f_weight_inh)) *
+                         static_cast<R>(ev);
     }
-    if (sic_refresh) n.I_sic = static_cast<R>(rc.w_a2n) * sic_sum;
+    if (sic_refresh) n.I_sic = as_r<R>(rc.w_a2n, rc.f_w_a2n) * sic_sum;
     R I_ext = n.I_sic;
     if (has_noise) I_ext += static_cast<R>(noise);
 
     double V = n.V, w = n.w;
-    R g_ex = n.g_ex, dg_ex = n.dg_ex + exc_input * static_cast<R>(pk.psc_init_ex);
-    R g_in = n.g_in, dg_in = n.dg_in + inh_input * static_cast<R>(pk.psc_init_in);
+    R g_ex = n.g_ex, dg_ex = n.dg_ex + exc_input * as_r<R>(pk.psc_init_ex, pk.f_psc_init_ex);
+    R g_in = n.g_in, dg_in = n.dg_in + inh_input * as_r<R>(pk.psc_init_in, pk.f_psc_init_in);
     int refractory = n.refr;
     bool spiked = false;
-    const R hs = static_cast<R>(rc.h_step);
+    const R hs = as_r<R>(rc.h_step, rc.f_h_step);
+    const R h6 = as_r<R>(rc.h6, rc.f_h6);
     for (int sub = 0; sub < rc.substeps; ++sub) {
         const R g_ex_next = ex_decay * (g_ex + hs * dg_ex);
         const R dg_ex_next = ex_decay * dg_ex;
@@ -208,10 +230,8 @@ __device__ __forceinline__ bool neuron_advance_step(const RunConsts& rc, const N
             neuron_rhs(pk, v + static_cast<R>(0.5) * hs * k2V, ww + static_cast<R>(0.5) * hs * k2w, g_ex_mid,
                           g_in_mid, I_ext, k3V, k3w);
             neuron_rhs(pk, v + hs * k3V, ww + hs * k3w, g_ex_next, g_in_next, I_ext, k4V, k4w);
-            V += static_cast<double>((hs / static_cast<R>(6.0)) *
-                                     (k1V + static_cast<R>(2.0) * k2V + static_cast<R>(2.0) * k3V + k4V));
-            w += static_cast<double>((hs / static_cast<R>(6.0)) *
-                                     (k1w + static_cast<R>(2.0) * k2w + static_cast<R>(2.0) * k3w + k4w));
+            V += static_cast<double>(h6 * (k1V + static_cast<R>(2.0) * k2V + static_cast<R>(2.0) * k3V + k4V));
+            w += static_cast<double>(h6 * (k1w + static_cast<R>(2.0) * k2w + static_cast<R>(2.0) * k3w + k4w));
         }
         g_ex = g_ex_next;
         dg_ex = dg_ex_next;
@@ -222,7 +242,7 @@ __device__ __forceinline__ bool neuron_advance_step(const RunConsts& rc, const N
         } else if (V >= pk.V_peak) {  // threshold test in double
             V = n.V_reset;
             w += n.b;
-            refractory = static_cast<int>(pk.t_ref / rc.h_step + 0.5);
+            refractory = pk.ref_steps;  // static_cast<int>(t_ref / h_step + 0.5)
             spiked = true;
         }
     }
@@ -295,7 +315,7 @@ __device__ __forceinline__ bool neuron_cell_step(const RunConsts& rc, const Step
     const double noise = has_noise ? neuron_noise<R>(rc, nstd, noise_idx, j) : 0.0;
     NeuronRegs<R> n{p.V[j], p.w[j], p.V_reset[j], p.b[j], p.g_ex[j], p.dg_ex[j], p.g_in[j], p.dg_in[j], p.I_sic[j],
                     p.refr[j]};
-    const R hs = static_cast<R>(rc.h_step);
+    const R hs = as_r<R>(rc.h_step, rc.f_h_step);
     const R ex_decay = exp_r(-hs / static_cast<R>(pk.tau_syn_ex));
     const R in_decay = exp_r(-hs / static_cast<R>(pk.tau_syn_in));
     const bool spiked = neuron_advance_step<R>(rc, pk, excitatory, n, exc_sum, inh_sum, sic_refresh, sic_sum,

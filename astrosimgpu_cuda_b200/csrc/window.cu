@@ -67,11 +67,6 @@ __global__ void gather_fwd_kernel(const u32* edge_idx, u64 n, const u32* row_of_
     if (pos) pos[i] = e - tgt_rs[r];
 }
 
-__global__ void max_fanout_kernel(const u32* rs, u32 n, unsigned* mx) {
-    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) atomicMax(mx, rs[i + 1] - rs[i]);
-}
-
 // Inverts a target-keyed CSR into a source-keyed one.  Within one source the
 // targets come out in increasing edge order (stable sort), which the push does not
 // depend on; positions let e2a deposits name their place in the target row.

@@ -87,88 +87,24 @@ __device__ __forceinline__ void pull_row(const u32* __restrict__ rs, const u32* 
     }
 }
 
-// One block of 128 cells advances through steps [s_begin, s_end) of the window that
-// starts at step win_start (buffer parity buf): block `blk` of the astrocytes when
-// `astro`, else block `blk` of the neurons.
-template <typename R>
-__device__ __forceinline__ void window_cells(const RunConsts& rc, const StepPtrs<R>& p, const WinPtrs<R>& w,
-                                             i64 win_start, int s_begin, int s_end, int buf, i64 mark, u32 blk,
-                                             bool astro) {
+// Neuron j through steps [s_begin, s_end) of the window starting at win_start.
+template <typename R, bool EXC>
+__device__ __forceinline__ void neuron_window(const RunConsts& rc, const NeuronK& pk, const StepPtrs<R>& p,
+                                              const WinPtrs<R>& w, u32 j, i64 win_start, int s_begin, int s_end,
+                                              int buf, bool pull, bool window_done) {
     const int prev = buf ^ 1;
     const int W = w.W;
-    const bool window_done = s_end == W;
-    const bool pull = w.mode[buf] != 0;
-    if (astro) {
-        // ------------------------------------------------------------ astrocytes
-        const u32 a = blk * blockDim.x + threadIdx.x;
-        const bool valid = a < rc.n_astro;
-        bool any_active = false;
-        if (valid) {
-            AstroRegs<R> s{p.Ca[a], p.IP3[a], p.h[a], p.Ca_tot[a], p.IP3_0[a], p.tau_IP3[a], p.delta_IP3[a]};
-            R acc[kMaxWindow];
-            const u64 slot_base = (static_cast<u64>(buf) * rc.n_astro + a);
-            const u32 c = w.ain_cnt[slot_base];
-            const bool ip3_input = pull || c > 0;
-            if (ip3_input)
-                for (int i = 0; i < W; ++i) acc[i] = static_cast<R>(0.0);
-            if (pull || c > kInboxSlots) {
-                pull_row<R>(p.e2a_rs, p.e2a_src, a, w.spk_word + static_cast<u64>(prev) * rc.n_neurons,
-                            w.spk_val + static_cast<u64>(prev) * W * rc.n_neurons, rc.n_neurons, s_begin, s_end, acc);
-            } else if (c > 0) {
-                Deposit<R> d[kInboxSlots];
-                for (u32 i = 0; i < c; ++i) d[i] = w.ain_ent[slot_base * kInboxSlots + i];
-                sort_deposits<R>(d, static_cast<int>(c));
-                for (u32 i = 0; i < c; ++i) {
-                    const int st = static_cast<int>(d[i].meta & 0xFFu);
-                    if (st >= s_begin && st < s_end) acc[st] += d[i].val;
-                }
-            }
-            if (window_done && c) w.ain_cnt[slot_base] = 0;
-            unsigned char ever = p.ever_active[a];
-            R* out = w.sic_win + (static_cast<u64>(buf) * rc.n_astro + a) * W;
-            R factor = static_cast<R>(0.0);
-            u64 pbase = step_base(rc.seed, kAstroPoissonKey, win_start + s_begin, a);
-            u64 nbase = step_base(rc.seed, kAstroNoiseKey, win_start + s_begin, a);
-            for (int st = s_begin; st < s_end; ++st) {
-                const i64 t = win_start + st;
-                factor = astro_advance_step<R>(rc, s, ip3_input ? acc[st] : static_cast<R>(0.0), a, t, pbase, nbase);
-                pbase += kStepAdvance;
-                nbase += kStepAdvance;
-                out[st] = factor;
-                if (factor > static_cast<R>(0.0)) {
-                    ever = 1;
-                    any_active = true;
-                }
-                if (t == mark) ever = 0;  // end of the pre-run (src/astrosim_fused.cu:1075)
-            }
-            p.Ca[a] = s.Ca;
-            p.IP3[a] = s.IP3;
-            p.h[a] = s.h;
-            p.ever_active[a] = ever;
-            p.sic_last[a] = factor;
-        }
-        const unsigned ballot = __ballot_sync(0xffffffffu, any_active);
-        if ((threadIdx.x & 31) == 0 && a < rc.n_astro) {
-            u32* word = w.astro_active + static_cast<u64>(buf) * w.astro_words + (a >> 5);
-            if (s_begin == 0) *word = ballot; else if (ballot) atomicOr(word, ballot);
-        }
-        return;
-    }
-    // ---------------------------------------------------------------- neurons
-    const u32 j = blk * blockDim.x + threadIdx.x;
-    if (j >= rc.n_neurons) return;
-    const bool excitatory = j < rc.n_exc;
-    const NeuronK& pk = excitatory ? rc.pe : rc.pi;
     const u64 nN = rc.n_neurons;
 
-    // synaptic input of the window: deposits (push) or the row walk (pull)
+    // synaptic input of the window: deposits (push) or the row walk (pull); steps
+    // whose bit in ex_mask / in_mask is clear have none (+0.0)
     R ex_acc[kMaxWindow], in_acc[kMaxWindow];
+    u32 ex_mask = 0, in_mask = 0;
     const u64 slot_base = static_cast<u64>(buf) * nN + j;
     const u32 c = w.nin_cnt[slot_base];
-    const bool syn_input = pull || c > 0;
-    if (syn_input)
-        for (int i = 0; i < W; ++i) ex_acc[i] = in_acc[i] = static_cast<R>(0.0);
     if (pull || c > kInboxSlots) {
+        for (int i = 0; i < W; ++i) ex_acc[i] = in_acc[i] = static_cast<R>(0.0);
+        ex_mask = in_mask = (1u << W) - 1u;
         const u32* words = w.spk_word + static_cast<u64>(prev) * nN;
         const R* vals = w.spk_val + static_cast<u64>(prev) * W * nN;
         pull_row<R>(p.exc_rs, p.exc_src, j, words, vals, nN, s_begin, s_end, ex_acc);
@@ -180,7 +116,14 @@ __device__ __forceinline__ void window_cells(const RunConsts& rc, const StepPtrs
         for (u32 i = 0; i < c; ++i) {
             const int st = static_cast<int>(d[i].meta & 0xFFu);
             if (st < s_begin || st >= s_end) continue;
-            if ((d[i].meta >> 8) == 0) ex_acc[st] += d[i].val; else in_acc[st] += d[i].val;
+            const u32 bit = 1u << st;
+            if ((d[i].meta >> 8) == 0) {
+                ex_acc[st] = ((ex_mask & bit) ? ex_acc[st] : static_cast<R>(0.0)) + d[i].val;
+                ex_mask |= bit;
+            } else {
+                in_acc[st] = ((in_mask & bit) ? in_acc[st] : static_cast<R>(0.0)) + d[i].val;
+                in_mask |= bit;
+            }
         }
     }
     if (window_done && c) w.nin_cnt[slot_base] = 0;
@@ -206,31 +149,40 @@ __device__ __forceinline__ void window_cells(const RunConsts& rc, const StepPtrs
 
     NeuronRegs<R> n{p.V[j], p.w[j], p.V_reset[j], p.b[j], p.g_ex[j], p.dg_ex[j], p.g_in[j], p.dg_in[j], p.I_sic[j],
                     p.refr[j]};
-    const R hs = static_cast<R>(rc.h_step);
+    const R hs = as_r<R>(rc.h_step, rc.f_h_step);
     const R ex_decay = exp_r(-hs / static_cast<R>(pk.tau_syn_ex));
     const R in_decay = exp_r(-hs / static_cast<R>(pk.tau_syn_in));
-    const double nstd = excitatory ? rc.noise_exc : rc.noise_inh;
+    const double nstd = EXC ? rc.noise_exc : rc.noise_inh;
     const bool has_noise = nstd > 0.0 && rc.independent_noise;
-    u64 noise_idx_cached = ~0ull;
+    // Per-step schedule by counters instead of divisions: the SIC refresh runs when
+    // (t - d_a2n) >= 0 and (t - d_a2n) % sic_interval == 0, the noise index is
+    // t / steps_per_noise (src/astrosim_fused.cu:1046-1050).
+    const i64 t0 = win_start + s_begin;
+    i64 since = t0 - rc.d_a2n;
+    const int si = rc.sic_interval, spn = rc.steps_per_noise;
+    int phase = static_cast<int>(((since % si) + si) % si);
+    u64 nidx = static_cast<u64>(t0 / spn);
+    int nphase = static_cast<int>(t0 % spn);
     double noise = 0.0;
-    u64 pbase = step_base(rc.seed, kNeuronPoissonKey, win_start + s_begin, j);
+    if (has_noise) noise = neuron_noise<R>(rc, nstd, nidx, j);
+    u64 pbase = step_base(rc.seed, kNeuronPoissonKey, t0, j);
     u32 word = 0;
     R* vout = w.spk_val + static_cast<u64>(buf) * W * nN;
     for (int st = s_begin; st < s_end; ++st) {
         const i64 t = win_start + st;
-        const bool refresh = (t - rc.d_a2n >= 0) && ((t - rc.d_a2n) % rc.sic_interval == 0);
-        if (has_noise) {
-            const u64 idx = static_cast<u64>(t / rc.steps_per_noise);
-            if (idx != noise_idx_cached) {
-                noise = neuron_noise<R>(rc, nstd, idx, j);
-                noise_idx_cached = idx;
-            }
-        }
+        const bool refresh = since >= 0 && phase == 0;
+        if (has_noise && nphase == 0 && st != s_begin) noise = neuron_noise<R>(rc, nstd, nidx, j);
         const R zero = static_cast<R>(0.0);
         const bool spiked = neuron_advance_step<R>(
-            rc, pk, excitatory, n, syn_input ? ex_acc[st] : zero, syn_input ? in_acc[st] : zero, refresh,
-            sic_input ? sic_acc[st] : zero, has_noise, noise, pbase, ex_decay, in_decay);
+            rc, pk, EXC, n, ((ex_mask >> st) & 1u) ? ex_acc[st] : zero, ((in_mask >> st) & 1u) ? in_acc[st] : zero,
+            refresh, sic_input ? sic_acc[st] : zero, has_noise, noise, pbase, ex_decay, in_decay);
         pbase += kStepAdvance;
+        ++since;
+        if (++phase == si) phase = 0;
+        if (++nphase == spn) {
+            nphase = 0;
+            ++nidx;
+        }
         if (spiked) {
             const R out = stp_on_spike<R>(rc, p.stp_x[j], p.stp_u[j], p.stp_t[j], t);
             vout[static_cast<u64>(st) * nN + j] = out;
@@ -251,6 +203,89 @@ __device__ __forceinline__ void window_cells(const RunConsts& rc, const StepPtrs
     p.refr[j] = n.refr;
     u32* sw = w.spk_word + slot_base;
     *sw = s_begin == 0 ? word : (*sw | word);
+}
+
+// One block of 128 cells advances through steps [s_begin, s_end) of the window that
+// starts at step win_start (buffer parity buf): block `blk` of the astrocytes when
+// `astro`, else block `blk` of the neurons.
+template <typename R>
+__device__ __forceinline__ void window_cells(const RunConsts& rc, const StepPtrs<R>& p, const WinPtrs<R>& w,
+                                             i64 win_start, int s_begin, int s_end, int buf, i64 mark, u32 blk,
+                                             bool astro) {
+    const int prev = buf ^ 1;
+    const int W = w.W;
+    const bool window_done = s_end == W;
+    const bool pull = w.mode[buf] != 0;
+    if (astro) {
+        // ------------------------------------------------------------ astrocytes
+        const u32 a = blk * blockDim.x + threadIdx.x;
+        const bool valid = a < rc.n_astro;
+        bool any_active = false;
+        if (valid) {
+            AstroRegs<R> s = load_astro<R>(p.Ca[a], p.IP3[a], p.h[a], p.Ca_tot[a], p.IP3_0[a], p.tau_IP3[a],
+                                           p.delta_IP3[a]);
+            // per-step IP3 input; steps whose bit in in_mask is clear have none (+0.0)
+            R acc[kMaxWindow];
+            u32 in_mask = 0;
+            const u64 slot_base = (static_cast<u64>(buf) * rc.n_astro + a);
+            const u32 c = w.ain_cnt[slot_base];
+            if (pull || c > kInboxSlots) {
+                for (int i = 0; i < W; ++i) acc[i] = static_cast<R>(0.0);
+                in_mask = (1u << W) - 1u;
+                pull_row<R>(p.e2a_rs, p.e2a_src, a, w.spk_word + static_cast<u64>(prev) * rc.n_neurons,
+                            w.spk_val + static_cast<u64>(prev) * W * rc.n_neurons, rc.n_neurons, s_begin, s_end, acc);
+            } else if (c > 0) {
+                Deposit<R> d[kInboxSlots];
+                for (u32 i = 0; i < c; ++i) d[i] = w.ain_ent[slot_base * kInboxSlots + i];
+                sort_deposits<R>(d, static_cast<int>(c));
+                for (u32 i = 0; i < c; ++i) {
+                    const int st = static_cast<int>(d[i].meta & 0xFFu);
+                    if (st < s_begin || st >= s_end) continue;
+                    const u32 bit = 1u << st;
+                    acc[st] = ((in_mask & bit) ? acc[st] : static_cast<R>(0.0)) + d[i].val;
+                    in_mask |= bit;
+                }
+            }
+            if (window_done && c) w.ain_cnt[slot_base] = 0;
+            unsigned char ever = p.ever_active[a];
+            R* out = w.sic_win + (static_cast<u64>(buf) * rc.n_astro + a) * W;
+            R factor = static_cast<R>(0.0);
+            u64 pbase = step_base(rc.seed, kAstroPoissonKey, win_start + s_begin, a);
+            u64 nbase = step_base(rc.seed, kAstroNoiseKey, win_start + s_begin, a);
+            for (int st = s_begin; st < s_end; ++st) {
+                const i64 t = win_start + st;
+                factor = astro_advance_step<R>(rc, s, ((in_mask >> st) & 1u) ? acc[st] : static_cast<R>(0.0), a, t,
+                                               pbase, nbase);
+                pbase += kStepAdvance;
+                nbase += kStepAdvance;
+                out[st] = factor;
+                if (factor > static_cast<R>(0.0)) {
+                    ever = 1;
+                    any_active = true;
+                }
+                if (t == mark) ever = 0;  // end of the pre-run (src/astrosim_fused.cu:1075)
+            }
+            p.Ca[a] = s.Ca;
+            p.IP3[a] = s.IP3;
+            p.h[a] = s.h;
+            p.ever_active[a] = ever;
+            p.sic_last[a] = factor;
+        }
+        const unsigned ballot = __ballot_sync(0xffffffffu, any_active);
+        if ((threadIdx.x & 31) == 0 && a < rc.n_astro) {
+            u32* word = w.astro_active + static_cast<u64>(buf) * w.astro_words + (a >> 5);
+            if (s_begin == 0) *word = ballot; else if (ballot) atomicOr(word, ballot);
+        }
+        return;
+    }
+    // ---------------------------------------------------------------- neurons
+    const u32 j = blk * blockDim.x + threadIdx.x;
+    if (j >= rc.n_neurons) return;
+    // one instantiation per population, so its constants are compile-time operands
+    if (j < rc.n_exc)
+        neuron_window<R, true>(rc, rc.pe, p, w, j, win_start, s_begin, s_end, buf, pull, window_done);
+    else
+        neuron_window<R, false>(rc, rc.pi, p, w, j, win_start, s_begin, s_end, buf, pull, window_done);
 }
 
 // After window `buf` completes: deliver its spikes into the inboxes of the next
