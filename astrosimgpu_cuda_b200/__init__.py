@@ -86,6 +86,9 @@ def lib():
     L.astrosim_server_result.argtypes = [S, C.c_uint64, C.POINTER(abi.RequestResult), C.POINTER(C.c_int)]
     L.astrosim_server_get_stats.argtypes = [S, C.POINTER(abi.ServerStats)]
     L.astrosim_server_destroy.argtypes = [S]
+    L.astrosim_selfcheck_division.argtypes = [C.c_int, C.POINTER(C.c_double), C.c_size_t, C.c_uint64, C.c_uint64,
+                                              C.POINTER(C.c_uint64)]
+    L.astrosim_selfcheck_division.restype = C.c_int
     for name in ("astrosim_server_create", "astrosim_server_submit", "astrosim_server_pump", "astrosim_server_result",
                  "astrosim_server_get_stats", "astrosim_server_destroy"):
         getattr(L, name).restype = C.c_int
@@ -102,6 +105,15 @@ def lib():
 def check(code):
     if code != abi.OK:
         raise AstrosimError(code, lib().astrosim_last_error().decode())
+
+
+def selfcheck_division(divisors, samples=1 << 20, seed=1, device=0):
+    """Mismatches between the FP64 path's division by a constant and IEEE x / y on the device."""
+    d = np.ascontiguousarray(divisors, dtype=np.float64)
+    out = C.c_uint64(0)
+    check(lib().astrosim_selfcheck_division(device, d.ctypes.data_as(C.POINTER(C.c_double)), d.size, samples, seed,
+                                            C.byref(out)))
+    return int(out.value)
 
 
 def _u32p(a):

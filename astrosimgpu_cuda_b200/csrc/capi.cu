@@ -362,3 +362,12 @@ extern "C" int astrosim_astro_totals_noalloc(const double* ca, const unsigned ch
                                       static_cast<cudaStream_t>(stream));
     });
 }
+
+namespace astrosim {
+Status selfcheck_division(int device, const double* divisors, size_t n, u64 samples, u64 seed, u64* mismatches);
+}
+
+extern "C" int astrosim_selfcheck_division(int device, const double* divisors, size_t n_divisors, uint64_t samples,
+                                           uint64_t seed, uint64_t* mismatches) {
+    return guarded([&] { return astrosim::selfcheck_division(device, divisors, n_divisors, samples, seed, mismatches); });
+}

@@ -165,6 +165,7 @@ struct AstroK {
     float f_inv_ratio, f_ratio_rate_IP3R, f_ratio_rate_L, f_k_Kd_inh, f_Km2;
     // Float copies read by the FP32 stages (converted once here, not per use).
     float f_Kd_IP3_1, f_Kd_IP3_2, f_Kd_act, f_rate_SERCA, f_k_IP3R, f_SIC_scale;
+    double rcp_ratio;  // RN(1 / ratio_ER_cyt), for the exact division by a constant (div_by)
 };
 
 // AdEx neuron constants for one population (src/astrosim_fused.cu:228-232).
@@ -182,6 +183,8 @@ struct NeuronK {
     // Refractory length in steps, static_cast<int>(t_ref / h_step + 0.5) (src/astrosim_fused.cu:555);
     // set with the step size.
     int ref_steps;
+    // RN(1 / x) of the constant divisors, for the exact division by a constant (div_by).
+    double rcp_C_m, rcp_tau_w, rcp_Delta_T;
 };
 
 // Biology defaults, compiled into the reference (src/astrosim_fused.cu:742-781).
@@ -235,6 +238,7 @@ inline AstroK astro_constants(const Biology& b) {  // src/astrosim_fused.cu:935-
     k.f_rate_SERCA = static_cast<float>(b.rate_SERCA);
     k.f_k_IP3R = static_cast<float>(b.k_IP3R);
     k.f_SIC_scale = static_cast<float>(b.SIC_scale);
+    k.rcp_ratio = 1.0 / b.ratio_ER_cyt;
     return k;
 }
 
@@ -274,6 +278,9 @@ inline NeuronK neuron_constants(const Biology& b, bool exc) {  // src/astrosim_f
     k.f_psc_init_ex = static_cast<float>(k.psc_init_ex);
     k.f_psc_init_in = static_cast<float>(k.psc_init_in);
     k.ref_steps = 0;
+    k.rcp_C_m = 1.0 / k.C_m;
+    k.rcp_tau_w = 1.0 / k.tau_w;
+    k.rcp_Delta_T = 1.0 / k.Delta_T;
     return k;
 }
 
@@ -282,43 +289,97 @@ inline int delay_to_steps(double delay_ms, double dt) {  // src/astrosim_fused.c
     return s < 1 ? 1 : s;
 }
 
-// ------------------------------------------------------------------ right-hand sides
-// Li-Rinzel: src/astrosim_fused.cu:236-253 (operand order kept).
-template <typename R>
-__host__ __device__ __forceinline__ void astro_rhs(const AstroK& c, R Ca_tot, R IP3_0, R tau_IP3, R Ca, R IP3, R h,
-                                                   R noise, R& dCa, R& dIP3, R& dh) {
-    const R ratio = static_cast<R>(c.ratio_ER_cyt);
-    const R Ca_ER = (Ca_tot - Ca) / ratio;
-    const R m_inf = IP3 / (IP3 + static_cast<R>(c.Kd_IP3_1));
-    const R n_inf = Ca / (Ca + static_cast<R>(c.Kd_act));
-    const R m3 = m_inf * m_inf * m_inf;
-    const R n3 = n_inf * n_inf * n_inf;
-    const R h3 = h * h * h;
-    const R J_channel = ratio * static_cast<R>(c.rate_IP3R) * m3 * n3 * h3 * (Ca_ER - Ca);
-    const R J_pump = static_cast<R>(c.rate_SERCA) * Ca * Ca /
-                     (static_cast<R>(c.Km_SERCA) * static_cast<R>(c.Km_SERCA) + Ca * Ca);
-    const R J_leak = ratio * static_cast<R>(c.rate_L) * (Ca_ER - Ca);
-    const R alpha_h = static_cast<R>(c.k_IP3R) * static_cast<R>(c.Kd_inh) * (IP3 + static_cast<R>(c.Kd_IP3_1)) /
-                      (IP3 + static_cast<R>(c.Kd_IP3_2));
-    const R beta_h = static_cast<R>(c.k_IP3R) * Ca;
-    dCa = J_channel - J_pump + J_leak + noise;
-    dIP3 = (IP3_0 - IP3) / tau_IP3;
-    dh = alpha_h * (static_cast<R>(1.0) - h) - beta_h * h;
+// ------------------------------------------------------------------ device arithmetic
+#ifdef __CUDACC__
+// Hardware approximations of the FP32 form, denormals flushed to zero:
+// exp(x) = 2^(x log2 e), log(x) = log2(x) ln 2, a / b = a * (1 / b).
+__device__ __forceinline__ float ex2_ftz(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
 }
+__device__ __forceinline__ float lg2_ftz(float x) {
+    float y;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rcp_ftz(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float sqrt_ftz(float x) {
+    float y;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float cos_ftz(float x) {
+    float y;
+    asm("cos.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+constexpr float kLog2E = 1.44269504088896340736f;  // log2(e)
+constexpr float kLn2 = 0.69314718055994530942f;    // ln(2)
+__device__ __forceinline__ float exp_fast(float x) { return ex2_ftz(x * kLog2E); }
+__device__ __forceinline__ float log_fast(float x) { return lg2_ftz(x) * kLn2; }
+__device__ __forceinline__ float div_fast(float a, float b) { return a * rcp_ftz(b); }
+
+// x / y rounded to nearest, for a divisor whose reciprocal ry = RN(1 / y) is known.
+// q0 = RN(x ry) is within 1.5 ulp of x / y; one correction q1 = RN(q0 + (x - q0 y) ry)
+// leaves an O(2^-106) relative error, so q1 is a faithful quotient; then by Markstein's
+// theorem (faithful q, correctly rounded ry => the remainder x - q y is exact and
+// RN(q + (x - q y) ry) = RN(x / y)) the second correction returns the rounded quotient.
+// Holds while x / y neither overflows nor underflows; x = -0 keeps its sign.
+__device__ __forceinline__ double div_by(double x, double y, double ry) {
+    double q = x * ry;
+    double r = fma(-q, y, x);
+    q = fma(r, ry, q);
+    r = fma(-q, y, x);
+    const double out = fma(r, ry, q);
+    return (__double_as_longlong(x) << 1) == 0 ? x : out;
+}
+#endif
+
+// ------------------------------------------------------------------ right-hand sides
+#ifdef __CUDACC__
+// Li-Rinzel: src/astrosim_fused.cu:236-253 (operand order kept; the divisions by the
+// constants ratio_ER_cyt and tau_IP3 are exact, see div_by; rcp_tau_IP3 = RN(1 / tau_IP3)).
+__device__ __forceinline__ void astro_rhs(const AstroK& c, double Ca_tot, double IP3_0, double tau_IP3,
+                                          double rcp_tau_IP3, double Ca, double IP3, double h, double noise,
+                                          double& dCa, double& dIP3, double& dh) {
+    const double ratio = c.ratio_ER_cyt;
+    const double Ca_ER = div_by(Ca_tot - Ca, ratio, c.rcp_ratio);
+    const double m_inf = IP3 / (IP3 + c.Kd_IP3_1);
+    const double n_inf = Ca / (Ca + c.Kd_act);
+    const double m3 = m_inf * m_inf * m_inf;
+    const double n3 = n_inf * n_inf * n_inf;
+    const double h3 = h * h * h;
+    const double J_channel = ratio * c.rate_IP3R * m3 * n3 * h3 * (Ca_ER - Ca);
+    const double J_pump = c.rate_SERCA * Ca * Ca / (c.Km_SERCA * c.Km_SERCA + Ca * Ca);
+    const double J_leak = ratio * c.rate_L * (Ca_ER - Ca);
+    const double alpha_h = c.k_IP3R * c.Kd_inh * (IP3 + c.Kd_IP3_1) / (IP3 + c.Kd_IP3_2);
+    const double beta_h = c.k_IP3R * Ca;
+    dCa = J_channel - J_pump + J_leak + noise;
+    dIP3 = div_by(IP3_0 - IP3, tau_IP3, rcp_tau_IP3);
+    dh = alpha_h * (1.0 - h) - beta_h * h;
+}
+#endif
 
 __device__ __forceinline__ double exp_r(double x) { return exp(x); }
 __device__ __forceinline__ float exp_r(float x) { return expf(x); }
 
-// AdEx: src/astrosim_fused.cu:281-290 (operand order kept).
+// AdEx: src/astrosim_fused.cu:281-290 (operand order kept; the divisions by the
+// constants C_m, tau_w and Delta_T are exact, see div_by).
 __device__ __forceinline__ void neuron_rhs(const NeuronK& p, double V, double w, double g_ex, double g_in,
                                            double I_ext, double& dV, double& dw) {
     const double Vc = V < p.V_peak ? V : p.V_peak;
-    const double arg = p.inv_Delta_T_pow2 != 0.0 ? (Vc - p.V_th) * p.inv_Delta_T_pow2 : (Vc - p.V_th) / p.Delta_T;
+    const double arg = p.inv_Delta_T_pow2 != 0.0 ? (Vc - p.V_th) * p.inv_Delta_T_pow2
+                                                 : div_by(Vc - p.V_th, p.Delta_T, p.rcp_Delta_T);
     const double I_spike = p.g_L * p.Delta_T * exp(arg);
     const double I_syn_ex = g_ex * (Vc - p.E_ex);
     const double I_syn_in = g_in * (Vc - p.E_in);
-    dV = (-p.g_L * (Vc - p.E_L) + I_spike - I_syn_ex - I_syn_in - w + p.I_e + I_ext) / p.C_m;
-    dw = (p.a * (Vc - p.E_L) - w) / p.tau_w;
+    dV = div_by(-p.g_L * (Vc - p.E_L) + I_spike - I_syn_ex - I_syn_in - w + p.I_e + I_ext, p.C_m, p.rcp_C_m);
+    dw = div_by(p.a * (Vc - p.E_L) - w, p.tau_w, p.rcp_tau_w);
 }
 
 // The FP32 form of the same right-hand side: reciprocal multiplies and the
@@ -326,7 +387,7 @@ __device__ __forceinline__ void neuron_rhs(const NeuronK& p, double V, double w,
 __device__ __forceinline__ void neuron_rhs(const NeuronK& p, float V, float w, float g_ex, float g_in, float I_ext,
                                            float& dV, float& dw) {
     const float Vc = V < p.f_V_peak ? V : p.f_V_peak;
-    const float I_spike = p.f_gL_DT * __expf((Vc - p.f_V_th) * p.f_inv_DT);
+    const float I_spike = p.f_gL_DT * exp_fast((Vc - p.f_V_th) * p.f_inv_DT);
     const float I_syn_ex = g_ex * (Vc - p.f_E_ex);
     const float I_syn_in = g_in * (Vc - p.f_E_in);
     dV = (-p.f_g_L * (Vc - p.f_E_L) + I_spike - I_syn_ex - I_syn_in - w + p.f_I_e + I_ext) * p.f_inv_Cm;
@@ -338,15 +399,15 @@ __device__ __forceinline__ void astro_rhs_fast(const AstroK& c, float Ca_tot, fl
                                                float Ca, float IP3, float h, float noise, float& dCa, float& dIP3,
                                                float& dh) {
     const float Ca_ER = (Ca_tot - Ca) * c.f_inv_ratio;
-    const float m_inf = __fdividef(IP3, IP3 + c.f_Kd_IP3_1);
-    const float n_inf = __fdividef(Ca, Ca + c.f_Kd_act);
+    const float m_inf = div_fast(IP3, IP3 + c.f_Kd_IP3_1);
+    const float n_inf = div_fast(Ca, Ca + c.f_Kd_act);
     const float m3 = m_inf * m_inf * m_inf;
     const float n3 = n_inf * n_inf * n_inf;
     const float h3 = h * h * h;
     const float J_channel = c.f_ratio_rate_IP3R * m3 * n3 * h3 * (Ca_ER - Ca);
-    const float J_pump = __fdividef(c.f_rate_SERCA * Ca * Ca, c.f_Km2 + Ca * Ca);
+    const float J_pump = div_fast(c.f_rate_SERCA * Ca * Ca, c.f_Km2 + Ca * Ca);
     const float J_leak = c.f_ratio_rate_L * (Ca_ER - Ca);
-    const float alpha_h = __fdividef(c.f_k_Kd_inh * (IP3 + c.f_Kd_IP3_1), IP3 + c.f_Kd_IP3_2);
+    const float alpha_h = div_fast(c.f_k_Kd_inh * (IP3 + c.f_Kd_IP3_1), IP3 + c.f_Kd_IP3_2);
     const float beta_h = c.f_k_IP3R * Ca;
     dCa = J_channel - J_pump + J_leak + noise;
     dIP3 = (IP3_0 - IP3) * inv_tau_IP3;
@@ -367,7 +428,7 @@ __device__ __forceinline__ float normal_fast(u64 base) {
     const u32 b = static_cast<u32>(rng_mix(base + kCounterMul) >> 40);
     const float u1 = (static_cast<float>(a) + 0.5f) * (1.0f / 16777216.0f);
     const float u2 = static_cast<float>(b) * (1.0f / 16777216.0f);
-    return sqrtf(-2.0f * __logf(u1)) * __cosf(static_cast<float>(kTwoPi) * u2);
+    return sqrt_ftz(-2.0f * log_fast(u1)) * cos_ftz(static_cast<float>(kTwoPi) * u2);
 }
 
 }  // namespace astrosim

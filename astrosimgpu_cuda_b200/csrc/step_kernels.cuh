@@ -50,13 +50,12 @@ __device__ __forceinline__ void astro_stage(const AstroK& c, R Ct, R I0, R tI, R
     if constexpr (std::is_same<R, float>::value) {
         astro_rhs_fast(c, Ct, I0, inv_tI, Ca, IP3, h, noise, dCa, dIP3, dh);
     } else {
-        (void)inv_tI;
-        astro_rhs<R>(c, Ct, I0, tI, Ca, IP3, h, noise, dCa, dIP3, dh);
+        astro_rhs(c, Ct, I0, tI, inv_tI, Ca, IP3, h, noise, dCa, dIP3, dh);
     }
 }
 
 __device__ __forceinline__ double log_r(double x) { return log(x); }
-__device__ __forceinline__ float log_r(float x) { return logf(x); }
+__device__ __forceinline__ float log_r(float x) { return log_fast(x); }
 
 // Register-resident state of one astrocyte.  The parameters are kept in double
 // (the accumulator updates and clamps use them) and in the stage type, converted
@@ -66,7 +65,7 @@ struct AstroRegs {
     double Ca, IP3;
     R h;
     double Ca_tot, IP3_0, tau_IP3, delta_IP3;
-    R Ct, I0, tI, inv_tI;  // stage copies of Ca_tot, IP3_0, tau_IP3 and 1 / tau_IP3 (FP32 form only)
+    R Ct, I0, tI, inv_tI;  // stage copies of Ca_tot, IP3_0, tau_IP3 and RN(1 / tau_IP3)
 };
 
 template <typename R>
@@ -83,7 +82,7 @@ __device__ __forceinline__ AstroRegs<R> load_astro(double Ca, double IP3, R h, d
     s.Ct = static_cast<R>(Ca_tot);
     s.I0 = static_cast<R>(IP3_0);
     s.tI = static_cast<R>(tau_IP3);
-    s.inv_tI = static_cast<R>(1.0) / s.tI;  // used by the FP32 form only
+    s.inv_tI = static_cast<R>(1.0) / s.tI;
     return s;
 }
 

@@ -143,7 +143,7 @@ namespace {
 // Launch-bounds variants the autotuner chooses from (minimum resident blocks of 128
 // threads per SM): more blocks trade registers (and a few spills) for occupancy.
 constexpr int kVariantsF32[] = {6, 8, 4};
-constexpr int kVariantsF64[] = {4, 6, 3};
+constexpr int kVariantsF64[] = {4, 5, 3};
 constexpr int kNumVariants = 3;
 constexpr int kTuneRounds = 2;
 
@@ -154,12 +154,18 @@ template <typename R>
 void launch_window(int variant, u32 grid, cudaStream_t st, const RunConsts& rc, const StepPtrs<R>& p,
                    const WinPtrs<R>& w, i64 start, int s0, int s1, int buf, i64 mark, u32 astro_blocks) {
     constexpr bool f32 = std::is_same<R, float>::value;
-    const int mb = f32 ? kVariantsF32[variant] : kVariantsF64[variant];
-    switch (mb) {
-        case 3: window_kernel<R, 3><<<grid, 128, 0, st>>>(rc, p, w, start, s0, s1, buf, mark, astro_blocks); break;
-        case 4: window_kernel<R, 4><<<grid, 128, 0, st>>>(rc, p, w, start, s0, s1, buf, mark, astro_blocks); break;
-        case 6: window_kernel<R, 6><<<grid, 128, 0, st>>>(rc, p, w, start, s0, s1, buf, mark, astro_blocks); break;
-        default: window_kernel<R, 8><<<grid, 128, 0, st>>>(rc, p, w, start, s0, s1, buf, mark, astro_blocks); break;
+    if constexpr (f32) {
+        switch (kVariantsF32[variant]) {
+            case 4: window_kernel<R, 4><<<grid, 128, 0, st>>>(rc, p, w, start, s0, s1, buf, mark, astro_blocks); break;
+            case 8: window_kernel<R, 8><<<grid, 128, 0, st>>>(rc, p, w, start, s0, s1, buf, mark, astro_blocks); break;
+            default: window_kernel<R, 6><<<grid, 128, 0, st>>>(rc, p, w, start, s0, s1, buf, mark, astro_blocks); break;
+        }
+    } else {
+        switch (kVariantsF64[variant]) {
+            case 3: window_kernel<R, 3><<<grid, 128, 0, st>>>(rc, p, w, start, s0, s1, buf, mark, astro_blocks); break;
+            case 5: window_kernel<R, 5><<<grid, 128, 0, st>>>(rc, p, w, start, s0, s1, buf, mark, astro_blocks); break;
+            default: window_kernel<R, 4><<<grid, 128, 0, st>>>(rc, p, w, start, s0, s1, buf, mark, astro_blocks); break;
+        }
     }
 }
 

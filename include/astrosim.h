@@ -316,6 +316,20 @@ typedef struct astrosim_astro_totals {
 int astrosim_astro_totals_noalloc(const double* ca, const unsigned char* engaged, uint32_t n_astro, double sic_th,
                                   astrosim_astro_totals* out, void* stream);
 
+/*
+ * Device arithmetic self-check: the FP64 right-hand sides divide by the model's
+ * constants (C_m, tau_w, Delta_T, ratio_ER_cyt and each astrocyte's tau_IP3) with a
+ * reciprocal and two FMA corrections instead of a hardware division sequence.
+ * This runs that division and IEEE x / y side by side on `device` for each of the
+ * `n_divisors` divisors over `samples` random dividends and `samples` dividends
+ * whose quotients lie next to a rounding midpoint, and writes the number of
+ * quotients that differ in any bit to *mismatches (0 on a correct device).
+ * Divisors must be finite, non-zero and have |x / y| in the normal range for the
+ * sampled x (|x| in [2^-40, 2^40]).  No counterpart in the reference.
+ */
+int astrosim_selfcheck_division(int device, const double* divisors, size_t n_divisors, uint64_t samples,
+                                uint64_t seed, uint64_t* mismatches);
+
 #ifdef __cplusplus
 }
 #endif
