@@ -9,6 +9,7 @@ the library's CUDA kernels.  There is no CPU path: importing works without a
 GPU, but creating a simulation needs the built library and a CUDA device.
 """
 import ctypes as C
+import json
 import math
 import os
 import subprocess
@@ -89,6 +90,23 @@ def lib():
     L.astrosim_selfcheck_division.argtypes = [C.c_int, C.POINTER(C.c_double), C.c_size_t, C.c_uint64, C.c_uint64,
                                               C.POINTER(C.c_uint64)]
     L.astrosim_selfcheck_division.restype = C.c_int
+    L.astrosim_record_calcium.argtypes = [P, C.c_int64, C.c_uint32, C.c_uint32, C.c_int64]
+    L.astrosim_calcium_samples.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    L.astrosim_copy_calcium.argtypes = [P, C.c_int64, C.c_int64, C.POINTER(C.c_double), C.c_int]
+    L.astrosim_sync.argtypes = [P]
+    L.astrosim_create_with_biology.argtypes = [C.POINTER(abi.Config), C.c_char_p, C.POINTER(P)]
+    L.astrosim_create_with_biology.restype = C.c_int
+    L.astrosim_biology_names.argtypes = [C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]
+    L.astrosim_biology_names.restype = C.c_int
+    L.astrosim_biology_value.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(C.c_double)]
+    L.astrosim_biology_value.restype = C.c_int
+    L.astrosim_ensemble_create_with_biology.argtypes = [C.POINTER(abi.Config), C.c_uint32, C.POINTER(C.c_char_p),
+                                                        C.POINTER(P)]
+    L.astrosim_ensemble_create_with_biology.restype = C.c_int
+    L.astrosim_server_submit_with_biology.argtypes = [P, C.POINTER(abi.Config), C.c_char_p, C.POINTER(C.c_uint64)]
+    L.astrosim_server_submit_with_biology.restype = C.c_int
+    for name in ("astrosim_record_calcium", "astrosim_calcium_samples", "astrosim_copy_calcium", "astrosim_sync"):
+        getattr(L, name).restype = C.c_int
     for name in ("astrosim_server_create", "astrosim_server_submit", "astrosim_server_pump", "astrosim_server_result",
                  "astrosim_server_get_stats", "astrosim_server_destroy"):
         getattr(L, name).restype = C.c_int
@@ -105,6 +123,30 @@ def lib():
 def check(code):
     if code != abi.OK:
         raise AstrosimError(code, lib().astrosim_last_error().decode())
+
+
+def _biology_json(biology):
+    if biology is None:
+        return None
+    if isinstance(biology, (str, bytes)):
+        return biology.encode() if isinstance(biology, str) else biology
+    return json.dumps(biology).encode()
+
+
+def biology_names():
+    """Names of the biology constants that astrosim_create_with_biology accepts."""
+    need = C.c_size_t()
+    check(lib().astrosim_biology_names(None, 0, C.byref(need)))
+    buf = C.create_string_buffer(need.value)
+    check(lib().astrosim_biology_names(buf, need.value, None))
+    return buf.value.decode().split(",")
+
+
+def biology_value(name, biology=None):
+    """A biology constant's value after `biology` overrides (defaults when None)."""
+    v = C.c_double()
+    check(lib().astrosim_biology_value(_biology_json(biology), name.encode(), C.byref(v)))
+    return v.value
 
 
 def selfcheck_division(divisors, samples=1 << 20, seed=1, device=0):
@@ -130,10 +172,11 @@ def device_info(device=0):
 class Simulation:
     """One network resident on the GPU (astrosim_create / step / summary / destroy)."""
 
-    def __init__(self, cfg=None, **overrides):
+    def __init__(self, cfg=None, biology=None, **overrides):
+        """`biology`: overrides of the biology constants, a {name: value} dict or JSON text."""
         self.cfg = cfg if cfg is not None else default_config(**overrides)
         self._h = C.c_void_p()
-        check(lib().astrosim_create(C.byref(self.cfg), C.byref(self._h)))
+        check(lib().astrosim_create_with_biology(C.byref(self.cfg), _biology_json(biology), C.byref(self._h)))
         n_exc, n_inh, n_astro, _ = scaling(self.cfg.n_total)
         self.n_exc, self.n_inh, self.n_astro = n_exc, n_inh, n_astro
         self.n_neurons = n_exc + n_inh
@@ -200,15 +243,40 @@ class Simulation:
     def dump_edges(self, path):
         check(lib().astrosim_dump_edges(self._h, os.fsencode(path)))
 
+    def record_calcium(self, every, first=0, n=None, max_samples=1024):
+        """Records Ca of astrocytes [first, first + n) after every `every`-th step, from the next step on."""
+        n = self.n_astro - first if n is None else n
+        check(lib().astrosim_record_calcium(self._h, int(every), int(first), int(n), int(max_samples)))
+        self._rec_n = n
+
+    def calcium_samples(self):
+        """(samples recorded so far, the step after which sample 0 was taken)."""
+        k, t0 = C.c_int64(), C.c_int64()
+        check(lib().astrosim_calcium_samples(self._h, C.byref(k), C.byref(t0)))
+        return k.value, t0.value
+
+    def calcium(self, first=0, n=None):
+        """Recorded samples [first, first + n) as an array [n, n_astro_recorded]."""
+        if n is None:
+            n = self.calcium_samples()[0] - first
+        out = np.empty((n, self._rec_n), dtype=np.float64)
+        check(lib().astrosim_copy_calcium(self._h, first, n, out.ctypes.data_as(C.POINTER(C.c_double)), 1))
+        return out
+
 
 class Ensemble:
     """Many independent networks stepped together (astrosim_ensemble_*)."""
 
-    def __init__(self, cfgs):
+    def __init__(self, cfgs, biology=None):
+        """`biology`: None, or one override (dict / JSON text / None) per network."""
         self.cfgs = list(cfgs)
         arr = (abi.Config * len(self.cfgs))(*self.cfgs)
         self._h = C.c_void_p()
-        check(lib().astrosim_ensemble_create(arr, len(self.cfgs), C.byref(self._h)))
+        if biology is None:
+            check(lib().astrosim_ensemble_create(arr, len(self.cfgs), C.byref(self._h)))
+        else:
+            texts = (C.c_char_p * len(self.cfgs))(*[_biology_json(b) for b in biology])
+            check(lib().astrosim_ensemble_create_with_biology(arr, len(self.cfgs), texts, C.byref(self._h)))
         self.sizes = [scaling(c.n_total) for c in self.cfgs]
 
     def close(self):
@@ -291,10 +359,10 @@ class Server:
         except Exception:
             pass
 
-    def submit(self, cfg=None, **overrides):
+    def submit(self, cfg=None, biology=None, **overrides):
         cfg = cfg if cfg is not None else default_config(precision=self.precision, **overrides)
         rid = C.c_uint64()
-        check(lib().astrosim_server_submit(self._h, C.byref(cfg), C.byref(rid)))
+        check(lib().astrosim_server_submit_with_biology(self._h, C.byref(cfg), _biology_json(biology), C.byref(rid)))
         return rid.value
 
     def pump(self, windows=10):

@@ -11,6 +11,7 @@
 #include <mutex>
 
 #include "../../include/astrosim.h"
+#include "biology.cuh"
 #include "ensemble.cuh"
 #include "reduce.cuh"
 #include "server.cuh"
@@ -84,6 +85,10 @@ const char* astrosim_last_error(void) { return g_last_error.c_str(); }
 int astrosim_abi_version(void) { return ASTROSIM_ABI_VERSION; }
 
 int astrosim_create(const astrosim_config* cfg, astrosim_handle** out) {
+    return astrosim_create_with_biology(cfg, nullptr, out);
+}
+
+int astrosim_create_with_biology(const astrosim_config* cfg, const char* biology_json, astrosim_handle** out) {
     if (!cfg || !out) return fail(ASTROSIM_ERR_INVALID_ARG, "null argument");
     *out = nullptr;
     if (cfg->struct_size != sizeof(astrosim_config))
@@ -96,7 +101,7 @@ int astrosim_create(const astrosim_config* cfg, astrosim_handle** out) {
     } catch (...) {
         return fail(ASTROSIM_ERR_OUT_OF_MEMORY, "host allocation failed");
     }
-    const int rc = guarded([&] { return h->sim.create(*cfg); });
+    const int rc = guarded([&] { return h->sim.create(*cfg, biology_json); });
     if (rc != ASTROSIM_OK) {
         const std::string msg = g_last_error;
         delete h;
@@ -159,7 +164,33 @@ int astrosim_last_step_ms(astrosim_handle* h, double* ms) {
     return guarded([&] { return h->sim.last_step_ms(ms); });
 }
 
+int astrosim_record_calcium(astrosim_handle* h, int64_t every_steps, uint32_t first_astro, uint32_t n_astro,
+                            int64_t max_samples) {
+    if (!h) return fail(ASTROSIM_ERR_INVALID_ARG, "null handle");
+    return guarded([&] { return h->sim.record_calcium(every_steps, first_astro, n_astro, max_samples); });
+}
+
+int astrosim_calcium_samples(astrosim_handle* h, int64_t* n_samples, int64_t* first_step) {
+    if (!h) return fail(ASTROSIM_ERR_INVALID_ARG, "null handle");
+    return guarded([&] { return h->sim.calcium_samples(n_samples, first_step); });
+}
+
+int astrosim_copy_calcium(astrosim_handle* h, int64_t first, int64_t n, double* dst, int wait) {
+    if (!h) return fail(ASTROSIM_ERR_INVALID_ARG, "null handle");
+    return guarded([&] { return h->sim.copy_calcium(first, n, dst, wait != 0); });
+}
+
+int astrosim_sync(astrosim_handle* h) {
+    if (!h) return fail(ASTROSIM_ERR_INVALID_ARG, "null handle");
+    return guarded([&] { return h->sim.sync(); });
+}
+
 int astrosim_ensemble_create(const astrosim_config* cfgs, uint32_t n_networks, astrosim_ensemble** out) {
+    return astrosim_ensemble_create_with_biology(cfgs, n_networks, nullptr, out);
+}
+
+int astrosim_ensemble_create_with_biology(const astrosim_config* cfgs, uint32_t n_networks,
+                                          const char* const* biology_json, astrosim_ensemble** out) {
     if (!cfgs || !out) return fail(ASTROSIM_ERR_INVALID_ARG, "null argument");
     *out = nullptr;
     for (uint32_t i = 0; i < n_networks; ++i) {
@@ -174,7 +205,7 @@ int astrosim_ensemble_create(const astrosim_config* cfgs, uint32_t n_networks, a
     } catch (...) {
         return fail(ASTROSIM_ERR_OUT_OF_MEMORY, "host allocation failed");
     }
-    const int rc = guarded([&] { return e->ens.create(cfgs, n_networks); });
+    const int rc = guarded([&] { return e->ens.create(cfgs, n_networks, biology_json); });
     if (rc != ASTROSIM_OK) {
         const std::string msg = g_last_error;
         delete e;
@@ -246,12 +277,17 @@ int astrosim_server_create(int device, int precision, uint64_t hbm_budget_bytes,
 }
 
 int astrosim_server_submit(astrosim_server* s, const astrosim_config* cfg, uint64_t* request_id) {
+    return astrosim_server_submit_with_biology(s, cfg, nullptr, request_id);
+}
+
+int astrosim_server_submit_with_biology(astrosim_server* s, const astrosim_config* cfg, const char* biology_json,
+                                        uint64_t* request_id) {
     if (!s || !cfg || !request_id) return fail(ASTROSIM_ERR_INVALID_ARG, "null argument");
     if (cfg->struct_size != sizeof(astrosim_config))
         return fail(ASTROSIM_ERR_INVALID_ARG, "astrosim_config.struct_size mismatch");
     return guarded([&] {
         astrosim::u64 id = 0;
-        astrosim::Status st = s->srv.submit(*cfg, &id);
+        astrosim::Status st = s->srv.submit(*cfg, &id, biology_json);
         *request_id = id;
         return st;
     });
@@ -370,4 +406,21 @@ Status selfcheck_division(int device, const double* divisors, size_t n, u64 samp
 extern "C" int astrosim_selfcheck_division(int device, const double* divisors, size_t n_divisors, uint64_t samples,
                                            uint64_t seed, uint64_t* mismatches) {
     return guarded([&] { return astrosim::selfcheck_division(device, divisors, n_divisors, samples, seed, mismatches); });
+}
+
+int astrosim_biology_names(char* buf, size_t cap, size_t* needed) {
+    const std::string names = astrosim::biology_names();
+    if (needed) *needed = names.size() + 1;
+    if (!buf) return ASTROSIM_OK;
+    if (cap < names.size() + 1) return fail(ASTROSIM_ERR_INVALID_ARG, "buffer too small for the name list");
+    std::memcpy(buf, names.c_str(), names.size() + 1);
+    return ASTROSIM_OK;
+}
+
+int astrosim_biology_value(const char* biology_json, const char* name, double* value) {
+    return guarded([&] {
+        astrosim::Biology b;
+        AS_TRY(astrosim::apply_biology_json(biology_json, b));
+        return astrosim::biology_get(b, name, value);
+    });
 }

@@ -2,13 +2,15 @@
 // lines (src/astrosim_fused.cu:791-1141), running on the C ABI of libastrosim_b200.
 //
 // Flags, defaults and the NaN "not overridden" sentinel follow
-// src/astrosim_fused.cu:792-844.  Two flags are added: --precision fp64|fp32 and
-// --device N.  The summary lines keep the reference's formats, which
+// src/astrosim_fused.cu:792-844.  Three flags are added: --precision fp64|fp32,
+// --device N and --biology FILE (a JSON object of biology constants).  The summary lines keep the reference's formats, which
 // scripts/run_gh200.sbatch:56-61 scrapes.  Differences: connectivity is built on the
 // GPU, so --dump-edges needs a device; the windowed-rate lines are printed at the
 // same steps from per-step spike counts.
 
 #include <algorithm>
+#include <fstream>
+#include <sstream>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -31,13 +33,15 @@ void print_help() {
         "astrosim --n N_total [--seed S] [--dt 0.1] [--substeps 1] "
         "[--pre-ms 1000] [--sim-ms 5000] [--block 128]\n"
         "         [--w-n2a W] [--w-a2n W] [--no-stp] [--dump-edges PATH]\n"
-        "         [--precision fp64|fp32] [--device N]\n"
+        "         [--precision fp64|fp32] [--device N] [--biology FILE.json]\n"
         "N_total is split by the fixed-in-degree scaling law: N_E=0.8*N, N_I=0.2*N,\n"
         "N_A=N/5, p_primary=80/N_E.  --w-n2a/--w-a2n override the neuron->astrocyte /\n"
         "astrocyte->neuron coupling weight (default 0.2 / 1.0); 0 disconnects that\n"
         "direction.  --no-stp disables Tsodyks-Markram short-term plasticity.\n"
         "--dump-edges PATH writes the network as type,source,target CSV and exits.\n"
         "--precision fp32 runs RK4 stages in float with double accumulators.\n"
+        "--biology FILE reads a JSON object of biology constants to override, e.g.\n"
+        "{\"exc_poiss_rate\": 3000, \"stp_U\": 0.4}; the flags above apply on top.\n"
         "Connectivity and every time step run on the GPU.\n");
 }
 
@@ -46,7 +50,7 @@ void print_help() {
 int main(int argc, char** argv) {
     astrosim_config cfg;
     astrosim_config_default(&cfg);
-    std::string dump_path;
+    std::string dump_path, biology;
     bool w_over = false;
     for (int i = 1; i < argc; ++i) {
         auto arg = [&](const char* name) { return std::strcmp(argv[i], name) == 0; };
@@ -68,6 +72,19 @@ int main(int argc, char** argv) {
             else if (v == "fp32" || v == "float") cfg.precision = ASTROSIM_PRECISION_FP32;
             else { std::fprintf(stderr, "unknown precision: %s\n", v.c_str()); return 1; }
         } else if (arg("--device")) cfg.device = std::atoi(next());
+        else if (arg("--biology")) {
+            const std::string path = next();
+            std::ifstream f(path);
+            if (!f) { std::fprintf(stderr, "cannot read %s for --biology\n", path.c_str()); return 1; }
+            std::stringstream ss;
+            ss << f.rdbuf();
+            biology = ss.str();
+            double probe = 0.0;
+            if (astrosim_biology_value(biology.c_str(), "w_e", &probe) != ASTROSIM_OK) {
+                std::fprintf(stderr, "--biology %s: %s\n", path.c_str(), astrosim_last_error());
+                return 1;
+            }
+        }
         else if (arg("--help") || arg("-h")) { print_help(); return 0; }
         else {
             std::fprintf(stderr, "unknown argument: %s (try --help)\n", argv[i]);
@@ -80,8 +97,9 @@ int main(int argc, char** argv) {
     const uint32_t n_inh = std::max<uint32_t>(1, n_total - n_exc);
     const uint32_t n_astro = std::max<uint32_t>(1, static_cast<uint32_t>(std::lround(n_total / 5.0)));
     const double p = std::min(1.0, 80.0 / static_cast<double>(n_exc));
-    const double w_n2a = std::isnan(cfg.w_n2a) ? 0.2 : cfg.w_n2a;
-    const double w_a2n = std::isnan(cfg.w_a2n) ? 1.0 : cfg.w_a2n;
+    double w_n2a = cfg.w_n2a, w_a2n = cfg.w_a2n;
+    if (std::isnan(w_n2a)) astrosim_biology_value(biology.c_str(), "w_n2a", &w_n2a);
+    if (std::isnan(w_a2n)) astrosim_biology_value(biology.c_str(), "w_a2n", &w_a2n);
     std::printf("=== astrosim: tripartite neuron-astrocyte network on B200 ===\n");
     std::printf("N_total=%u  N_E=%u  N_I=%u  N_A=%u  p_primary=%.6g  (fixed in-degree law, K_SYN=%.0f)\n", n_total,
                 n_exc, n_inh, n_astro, p, 80.0);
@@ -92,7 +110,7 @@ int main(int argc, char** argv) {
     std::fflush(stdout);
 
     astrosim_handle* h = nullptr;
-    if (astrosim_create(&cfg, &h) != ASTROSIM_OK) {
+    if (astrosim_create_with_biology(&cfg, biology.empty() ? nullptr : biology.c_str(), &h) != ASTROSIM_OK) {
         if (std::strstr(astrosim_last_error(), "no CUDA device")) {
             std::fprintf(stderr, "No CUDA device visible: connectivity and stepping run on the GPU.\n");
             return 1;

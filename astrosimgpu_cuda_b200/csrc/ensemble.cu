@@ -129,7 +129,7 @@ Status Ensemble::init_empty(bool fp32, int window, int device) {
     return Status::Ok();
 }
 
-Status Ensemble::create(const astrosim_config* cfgs, u32 n) {
+Status Ensemble::create(const astrosim_config* cfgs, u32 n, const char* const* biology_json) {
     if (!cfgs || n == 0) return make_error(ASTROSIM_ERR_INVALID_ARG, "an ensemble needs at least one network");
     for (u32 i = 1; i < n; ++i) {
         if (cfgs[i].dt != cfgs[0].dt || cfgs[i].substeps != cfgs[0].substeps ||
@@ -148,7 +148,7 @@ Status Ensemble::create(const astrosim_config* cfgs, u32 n) {
     auto work = [&] {
         for (u32 i = next++; i < n; i = next++) {
             auto s = std::make_unique<Simulation>();
-            st[i] = s->create(cfgs[i]);
+            st[i] = s->create(cfgs[i], biology_json ? biology_json[i] : nullptr);
             nets_[i] = std::move(s);
         }
     };

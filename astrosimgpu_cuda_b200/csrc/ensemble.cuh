@@ -20,7 +20,7 @@ namespace astrosim {
 class Ensemble {
 public:
     ~Ensemble();
-    Status create(const astrosim_config* cfgs, u32 n);
+    Status create(const astrosim_config* cfgs, u32 n, const char* const* biology_json = nullptr);
     Status step(i64 n_steps);
     Status summary(u32 i, astrosim_summary_t& out);
     Status get_state(u32 i, int which, double* dst, size_t count);

@@ -19,6 +19,7 @@
 #include <thread>
 #include <vector>
 
+#include "biology.cuh"
 #include "ensemble.cuh"
 #include "server.cuh"
 
@@ -90,7 +91,7 @@ void Server::builder_loop() {
         }
         const double tb = now_s();
         auto sim = std::make_unique<Simulation>();
-        Status s = sim->create(r->cfg);
+        Status s = sim->create(r->cfg, r->biology.empty() ? nullptr : r->biology.c_str());
         std::lock_guard<std::mutex> lk(mu_);
         --n_inflight_;
         r->build_s = now_s() - tb;
@@ -108,12 +109,17 @@ void Server::builder_loop() {
     }
 }
 
-Status Server::submit(const astrosim_config& cfg, u64* id) {
+Status Server::submit(const astrosim_config& cfg, u64* id, const char* biology_json) {
     if (cfg.dt != 0.1 || cfg.substeps < 1 || cfg.precision != precision_)
         return make_error(ASTROSIM_ERR_INVALID_ARG, "requests must use dt 0.1 ms and the server's precision");
     auto r = std::make_shared<Request>();
     r->cfg = cfg;
     r->cfg.device = device_;
+    if (biology_json) {
+        Biology check;  // reject bad overrides at submission, not in a builder thread
+        AS_TRY(apply_biology_json(biology_json, check));
+        r->biology = biology_json;
+    }
     r->bytes = estimate_bytes(cfg);
     if (r->bytes > budget_)
         return make_error(ASTROSIM_ERR_OUT_OF_MEMORY, "request needs about %llu bytes, more than the budget",

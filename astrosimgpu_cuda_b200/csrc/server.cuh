@@ -1,6 +1,8 @@
 // server.cuh -- continuous-batching request loop over the ensemble engine.
 #pragma once
 
+#include <string>
+
 #include <condition_variable>
 #include <deque>
 #include <map>
@@ -19,7 +21,7 @@ class Server {
 public:
     ~Server();
     Status create(int device, int precision, u64 budget_bytes, int builder_threads);
-    Status submit(const astrosim_config& cfg, u64* id);
+    Status submit(const astrosim_config& cfg, u64* id, const char* biology_json = nullptr);
     Status pump(i64 windows);
     Status result(u64 id, astrosim_request_result& out, bool* done);
     void stats(astrosim_server_stats& s);
@@ -29,6 +31,7 @@ private:
     struct Request {
         u64 id = 0;
         astrosim_config cfg{};
+        std::string biology;  // JSON overrides of the biology constants ("" = none)
         u64 bytes = 0;
         double submit_t = 0, admit_t = 0, start_t = 0, done_t = 0, build_s = 0;
         std::unique_ptr<Simulation> sim;

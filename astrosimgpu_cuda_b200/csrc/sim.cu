@@ -9,6 +9,7 @@
 #include <fstream>
 #include <vector>
 
+#include "biology.cuh"
 #include "sim.cuh"
 #include "step_kernels.cuh"
 #include "window.cuh"
@@ -81,8 +82,7 @@ __global__ void init_state_kernel(StepPtrs<R> p, RunConsts rc, double V_e, doubl
     }
 }
 
-Biology biology_for(const astrosim_config& cfg) {
-    Biology b;
+Biology biology_for(const astrosim_config& cfg, Biology b) {
     if (b.noise_dt <= 0.0) b.noise_dt = 10.0 * cfg.dt;  // src/astrosim_fused.cu:848
     if (!std::isnan(cfg.w_n2a)) b.w_n2a = cfg.w_n2a;
     if (!std::isnan(cfg.w_a2n)) b.w_a2n = cfg.w_a2n;
@@ -125,7 +125,7 @@ Simulation::~Simulation() {
     }
 }
 
-Status Simulation::create(const astrosim_config& cfg) {
+Status Simulation::create(const astrosim_config& cfg, const char* biology_json) {
     if (cfg.n_total == 0) return make_error(ASTROSIM_ERR_INVALID_ARG, "n_total must be >= 1");
     if (!(cfg.dt > 0.0) || !std::isfinite(cfg.dt)) return make_error(ASTROSIM_ERR_INVALID_ARG, "dt must be > 0");
     if (cfg.substeps < 1) return make_error(ASTROSIM_ERR_INVALID_ARG, "substeps must be >= 1");
@@ -154,7 +154,11 @@ Status Simulation::create(const astrosim_config& cfg) {
     keep_pool_memory(device_, 8ull << 30);
     AllocStream alloc_scope(stream_);
 
-    bio_ = biology_for(cfg);
+    {
+        Biology base;  // the reference's constants, then the JSON overrides, then cfg's fields
+        AS_TRY(apply_biology_json(biology_json, base));
+        bio_ = biology_for(cfg, base);
+    }
     const Sizes sz = scaling_law(cfg.n_total);
     BuildOptions bo;
     AS_TRY(build_network(sz, cfg.seed, bio_, bo, net_, stream_));
@@ -320,6 +324,58 @@ Status Simulation::step(i64 n) {
     steps_done_ += n;
     AS_CUDA(cudaStreamSynchronize(stream_));
     run_seconds_ += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return Status::Ok();
+}
+
+Status Simulation::record_calcium(i64 every, u32 first, u32 n, i64 max_samples) {
+    if (every < 1) return make_error(ASTROSIM_ERR_INVALID_ARG, "every_steps must be >= 1");
+    if (n == 0 || first >= rc_.n_astro || n > rc_.n_astro - first)
+        return make_error(ASTROSIM_ERR_INVALID_ARG, "astrocytes [%u, %u + %u) not in [0, %u)", first, first, n,
+                          rc_.n_astro);
+    if (max_samples < 1) return make_error(ASTROSIM_ERR_INVALID_ARG, "max_samples must be >= 1");
+    AS_CUDA(cudaSetDevice(device_));
+    AS_CUDA(cudaStreamSynchronize(stream_));
+    AllocStream alloc_scope(stream_);
+    DevBuf<double> buf;
+    AS_TRY(buf.alloc(static_cast<size_t>(max_samples) * n));
+    st_.ca_rec = std::move(buf);
+    st_.rec_every = every;
+    st_.rec_k0 = (steps_done_ + every) / every;  // first sample ends the first interval after steps_done_
+    st_.rec_cap = max_samples;
+    st_.rec_first = first;
+    st_.rec_n = n;
+    return Status::Ok();
+}
+
+Status Simulation::calcium_samples(i64* n_samples, i64* first_step) {
+    if (!st_.rec_n) return make_error(ASTROSIM_ERR_STATE, "calcium recording is off");
+    const i64 last = steps_done_ / st_.rec_every;  // last interval completed
+    i64 k = last - st_.rec_k0 + 1;
+    k = k < 0 ? 0 : (k > st_.rec_cap ? st_.rec_cap : k);
+    if (n_samples) *n_samples = k;
+    if (first_step) *first_step = st_.rec_k0 * st_.rec_every - 1;
+    return Status::Ok();
+}
+
+Status Simulation::copy_calcium(i64 first, i64 n, double* dst, bool wait) {
+    i64 have = 0;
+    AS_TRY(calcium_samples(&have, nullptr));
+    if (first < 0 || n < 0 || first + n > have)
+        return make_error(ASTROSIM_ERR_INVALID_ARG, "samples [%lld, %lld) not recorded (have %lld)",
+                          static_cast<long long>(first), static_cast<long long>(first + n),
+                          static_cast<long long>(have));
+    if (n == 0) return Status::Ok();
+    if (!dst) return make_error(ASTROSIM_ERR_INVALID_ARG, "null destination");
+    AS_CUDA(cudaSetDevice(device_));
+    AS_CUDA(cudaMemcpyAsync(dst, st_.ca_rec.get() + static_cast<u64>(first) * st_.rec_n,
+                            static_cast<size_t>(n) * st_.rec_n * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    if (wait) AS_CUDA(cudaStreamSynchronize(stream_));
+    return Status::Ok();
+}
+
+Status Simulation::sync() {
+    AS_CUDA(cudaSetDevice(device_));
+    AS_CUDA(cudaStreamSynchronize(stream_));
     return Status::Ok();
 }
 

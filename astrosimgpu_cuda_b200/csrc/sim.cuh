@@ -61,11 +61,17 @@ struct StateBuffers {
     DevBuf<u32> counts;            // spikes per step
     DevBuf<u32> raster;            // [raster_steps][words]
     DevBuf<unsigned char> reduce_raw;  // summary reduction partials + totals
+    // Calcium recording: sample k (0-based) is the Ca of astrocytes [rec_first,
+    // rec_first + rec_n) after step t = (rec_k0 + k) * rec_every - 1; [rec_cap][rec_n].
+    DevBuf<double> ca_rec;
+    i64 rec_every = 0, rec_k0 = 0, rec_cap = 0;
+    u32 rec_first = 0, rec_n = 0;
 };
 
 class Simulation {
 public:
-    Status create(const astrosim_config& cfg);
+    // biology_json: optional overrides of the biology constants (see apply_biology_json)
+    Status create(const astrosim_config& cfg, const char* biology_json = nullptr);
     Status step(i64 n);
     Status summary(astrosim_summary_t& out);
     Status spike_counts(i64 first, i64 n, u32* dst);
@@ -74,6 +80,10 @@ public:
     Status get_csr(int which, u32* rs, size_t rs_cap, u32* src, size_t src_cap, u32* n_targets, u64* n_edges);
     Status dump_edges(const char* path);
     Status last_step_ms(double* ms);
+    Status record_calcium(i64 every, u32 first, u32 n, i64 max_samples);
+    Status calcium_samples(i64* n_samples, i64* first_step);
+    Status copy_calcium(i64 first, i64 n, double* dst, bool wait);
+    Status sync();
     ~Simulation();
 
     const Sizes& sizes() const { return net_.sz; }

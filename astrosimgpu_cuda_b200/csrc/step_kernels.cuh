@@ -26,7 +26,20 @@ struct StepPtrs {
     i64 raster_steps;
     const double *Ca_tot, *IP3_0, *tau_IP3, *delta_IP3, *V_reset, *b;
     const u32 *exc_rs, *exc_src, *inh_rs, *inh_src, *sic_rs, *sic_src, *e2a_rs, *e2a_src;
+    double* ca_rec;  // calcium recording (null = off): [rec_cap][rec_n]
+    i64 rec_every, rec_k0, rec_cap;
+    u32 rec_first, rec_n;
 };
+
+// Stores astrocyte a's calcium as sample (t + 1) / rec_every - rec_k0 when step t
+// ends a recording interval and the sample fits.  `due` = ((t + 1) % rec_every == 0).
+template <typename R>
+__device__ __forceinline__ void record_ca(const StepPtrs<R>& p, u32 a, i64 t, bool due, double ca) {
+    const u32 i = a - p.rec_first;
+    if (!due || i >= p.rec_n) return;
+    const i64 k = (t + 1) / p.rec_every - p.rec_k0;
+    if (k >= 0 && k < p.rec_cap) p.ca_rec[static_cast<u64>(k) * p.rec_n + i] = ca;
+}
 
 // Sum of the delayed spike values of one CSR row, in row order, reading the packed
 // bit ring first and the value ring only for sources that spiked.  Skipped terms are
@@ -165,6 +178,7 @@ __device__ __forceinline__ void astro_cell_step(const RunConsts& rc, const StepP
     p.Ca[a] = s.Ca;
     p.IP3[a] = s.IP3;
     p.h[a] = s.h;
+    if (p.ca_rec) record_ca<R>(p, a, step, (step + 1) % p.rec_every == 0, s.Ca);
     if (factor > static_cast<R>(0.0)) p.ever_active[a] = 1;
     p.sic_ring[static_cast<u64>(step % S) * rc.n_astro + a] = factor;
     p.sic_last[a] = factor;
@@ -375,6 +389,12 @@ inline StepPtrs<R> make_ptrs(StateBuffers& s, Network& n, const RunConsts& rc, i
     p.sic_src = n.sic.src.get();
     p.e2a_rs = n.e2a.row_start.get();
     p.e2a_src = n.e2a.src.get();
+    p.ca_rec = s.rec_n ? s.ca_rec.get() : nullptr;
+    p.rec_every = s.rec_every;
+    p.rec_k0 = s.rec_k0;
+    p.rec_cap = s.rec_cap;
+    p.rec_first = s.rec_first;
+    p.rec_n = s.rec_n;
     return p;
 }
 

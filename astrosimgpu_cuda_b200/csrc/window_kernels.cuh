@@ -252,12 +252,18 @@ __device__ __forceinline__ void window_cells(const RunConsts& rc, const StepPtrs
             R factor = static_cast<R>(0.0);
             u64 pbase = step_base(rc.seed, kAstroPoissonKey, win_start + s_begin, a);
             u64 nbase = step_base(rc.seed, kAstroNoiseKey, win_start + s_begin, a);
+            // recording phase (t + 1) % rec_every, advanced by a counter
+            i64 rphase = p.ca_rec ? (win_start + s_begin + 1) % p.rec_every : 1;
             for (int st = s_begin; st < s_end; ++st) {
                 const i64 t = win_start + st;
                 factor = astro_advance_step<R>(rc, s, ((in_mask >> st) & 1u) ? acc[st] : static_cast<R>(0.0), a, t,
                                                pbase, nbase);
                 pbase += kStepAdvance;
                 nbase += kStepAdvance;
+                if (p.ca_rec) {
+                    record_ca<R>(p, a, t, rphase == 0, s.Ca);
+                    if (++rphase == p.rec_every) rphase = 0;
+                }
                 out[st] = factor;
                 if (factor > static_cast<R>(0.0)) {
                     ever = 1;

@@ -110,6 +110,31 @@ int astrosim_abi_version(void);
 int astrosim_create(const astrosim_config* cfg, astrosim_handle** out);
 
 /*
+ * astrosim_create with non-default biology.  `biology_json` is one flat JSON
+ * object mapping parameter names to values, e.g.
+ *     {"exc_poiss_rate": 3000, "stp_U": 0.4, "independent_noise": true}
+ * The names are the reference's biology constants (its Biology struct,
+ * src/astrosim_fused.cu:742-781; astrosim_biology_names lists them); reals and
+ * integers take numbers, flags take true / false.  The reference compiles these
+ * constants in; upstream loads them from a JSON config (not part of the
+ * reference).  cfg's own fields apply on top: w_n2a / w_a2n when not NaN,
+ * stp_enabled = 0, neuron_drive_scale (multiplies the neuron Poisson rates).
+ * NULL or "" keeps every default.  Unknown or repeated names, malformed text and
+ * values the model cannot run with (a non-positive time constant, capacitance or
+ * delay, sic_interval < 1, ...) return ASTROSIM_ERR_INVALID_ARG with the name in
+ * astrosim_last_error().  Delays that are not all equal, or not 2-16 steps, run on
+ * the per-step engine instead of the windowed one.
+ */
+int astrosim_create_with_biology(const astrosim_config* cfg, const char* biology_json, astrosim_handle** out);
+
+/* Comma-separated biology parameter names into buf (cap bytes, NUL included);
+   *needed (if not NULL) receives the size the list needs.  buf = NULL only sizes. */
+int astrosim_biology_names(char* buf, size_t cap, size_t* needed);
+
+/* The value of parameter `name` after applying biology_json (NULL = defaults). */
+int astrosim_biology_value(const char* biology_json, const char* name, double* value);
+
+/*
  * Advances the network by n_steps time steps, asynchronously on the handle's
  * stream.  Replaces the body of the reference time loop
  * (src/astrosim_fused.cu:1042-1102): the per-step scalars, the astrocyte and
@@ -195,6 +220,33 @@ int astrosim_dump_edges(astrosim_handle* h, const char* path);
 int astrosim_last_step_ms(astrosim_handle* h, double* ms);
 
 /*
+ * Calcium recording into device memory (the reference records nothing beyond its
+ * printed summary; upstream recording is out of its scope, README.md:120-123).
+ * From the next step on, after every step t with (t + 1) % every_steps == 0, the
+ * kernels store the calcium of astrocytes [first_astro, first_astro + n_astro) as
+ * one sample (n_astro doubles) in a device buffer of max_samples samples; samples
+ * past the buffer are dropped.  Starting a recording replaces the previous one and
+ * its buffer.  Recording adds no launches: the astrocyte update writes the sample.
+ */
+int astrosim_record_calcium(astrosim_handle* h, int64_t every_steps, uint32_t first_astro, uint32_t n_astro,
+                            int64_t max_samples);
+
+/* Samples recorded so far (at most max_samples) and the step after which sample 0 was taken. */
+int astrosim_calcium_samples(astrosim_handle* h, int64_t* n_samples, int64_t* first_step);
+
+/*
+ * Copies samples [first, first + n) to dst (n * n_astro doubles, sample-major).
+ * wait = 1 returns once the copy is done.  wait = 0 enqueues the copy on the
+ * handle's stream and returns at once; the data is in dst after astrosim_sync
+ * (or any call that synchronises the handle).  Pinned host memory lets the copy
+ * overlap host work.
+ */
+int astrosim_copy_calcium(astrosim_handle* h, int64_t first, int64_t n, double* dst, int wait);
+
+/* Waits for everything enqueued on the handle's stream. */
+int astrosim_sync(astrosim_handle* h);
+
+/*
  * Name and compute capability of a CUDA device (the reference prints them after
  * its device check, src/astrosim_fused.cu:904-914).  Returns ASTROSIM_ERR_NO_DEVICE
  * when no device is visible.
@@ -214,6 +266,12 @@ typedef struct astrosim_ensemble astrosim_ensemble;
 
 /* Builds every network (concurrently) and its state. */
 int astrosim_ensemble_create(const astrosim_config* cfgs, uint32_t n_networks, astrosim_ensemble** out);
+
+/* Same, with biology overrides per network (biology_json[i] as in astrosim_create_with_biology;
+   the array or any entry may be NULL).  All networks must still share one window length:
+   equal delays d_e = d_i = d_a2n. */
+int astrosim_ensemble_create_with_biology(const astrosim_config* cfgs, uint32_t n_networks,
+                                          const char* const* biology_json, astrosim_ensemble** out);
 
 /* Advances every network by n_steps (a whole number of windows, 1 ms each); a
    network stops at its own pre_ms + sim_ms. */
@@ -266,6 +324,9 @@ typedef struct astrosim_server_stats {
 int astrosim_server_create(int device, int precision, uint64_t hbm_budget_bytes, int builder_threads,
                            astrosim_server** out);
 int astrosim_server_submit(astrosim_server* s, const astrosim_config* cfg, uint64_t* request_id);
+/* Same, with biology overrides (checked here; the text is copied). */
+int astrosim_server_submit_with_biology(astrosim_server* s, const astrosim_config* cfg, const char* biology_json,
+                                        uint64_t* request_id);
 /* Admits what fits, joins built networks, advances the batch by `windows` windows
    (1 ms each) and retires finished requests. */
 int astrosim_server_pump(astrosim_server* s, int64_t windows);

@@ -671,6 +671,45 @@ void oracle_seq_normals(uint64_t seed, uint64_t stream, size_t n, double* out) {
     for (size_t i = 0; i < n; ++i) out[i] = rs.next_normal();
 }
 
+// Sets Bio fields by name (the same names as the reference's Biology struct,
+// src/astrosim_fused.cu:742-781): numbers for reals and sic_interval, 0/1 for flags.
+static bool set_bio(Bio& b, const char* name, double v) {
+#define R_(f) if (std::strcmp(name, #f) == 0) { b.f = v; return true; }
+#define F_(f) if (std::strcmp(name, #f) == 0) { b.f = v != 0.0; return true; }
+    R_(Ca_tot) R_(IP3_0) R_(tau_IP3) R_(delta_IP3) R_(SIC_scale) R_(Kd_IP3_1) R_(Kd_IP3_2) R_(Kd_act) R_(Kd_inh)
+    R_(Km_SERCA) R_(SIC_th) R_(k_IP3R) R_(rate_IP3R) R_(rate_L) R_(rate_SERCA) R_(ratio_ER_cyt) R_(Ca_init)
+    R_(h_init) R_(IP3_init) F_(randomize_astro) R_(ra_lower) R_(ra_upper) R_(ra_var)
+    R_(e_Delta_T) R_(e_a) R_(e_tau_w) R_(e_V_reset) R_(e_b) R_(e_V_m) R_(e_C_m) R_(e_g_L) R_(e_E_L) R_(e_V_th)
+    R_(e_V_peak) R_(e_t_ref) R_(e_E_ex) R_(e_E_in) R_(e_tau_syn_ex) R_(e_tau_syn_in)
+    R_(i_Delta_T) R_(i_a) R_(i_tau_w) R_(i_V_reset) R_(i_b) R_(i_V_m) R_(i_C_m) R_(i_g_L) R_(i_E_L) R_(i_V_th)
+    R_(i_V_peak) R_(i_t_ref) R_(i_E_ex) R_(i_E_in) R_(i_tau_syn_ex) R_(i_tau_syn_in)
+    F_(randomize_neuron) R_(rn_lower) R_(rn_upper) R_(rn_var) R_(w_e) R_(w_i) R_(w_n2a) R_(w_a2n)
+    R_(d_e) R_(d_i) R_(d_a2n) F_(stp_enabled) R_(stp_U) R_(stp_tau_rec) R_(stp_tau_fac)
+    R_(astro_poiss_rate) R_(astro_poiss_weight) R_(astro_noise_std) R_(exc_poiss_rate) R_(exc_poiss_weight)
+    R_(exc_noise_std) R_(inh_poiss_rate) R_(inh_poiss_weight) R_(inh_noise_std) F_(independent_noise) R_(noise_dt)
+#undef R_
+#undef F_
+    if (std::strcmp(name, "sic_interval") == 0) { b.sic_interval = static_cast<int>(v); return true; }
+    return false;
+}
+
+oracle_sim* oracle_create_with_biology(const astrosim_config* cfg, int n_threads, const char* const* names,
+                                       const double* values, size_t n) {
+    oracle_sim* s = make_sim(cfg, n_threads);
+    if (!s) return nullptr;
+    for (size_t i = 0; i < n; ++i) {
+        if (!set_bio(s->bio, names[i], values[i])) {
+            delete s;
+            return nullptr;
+        }
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    s->net = build_network(s->sz, cfg->seed);
+    s->build_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    init_state(s);
+    return s;
+}
+
 oracle_sim* oracle_create(const astrosim_config* cfg, int n_threads) {
     oracle_sim* s = make_sim(cfg, n_threads);
     if (!s) return nullptr;

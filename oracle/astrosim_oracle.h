@@ -50,6 +50,14 @@ oracle_sim* oracle_create_with_csr(const astrosim_config* cfg, int n_threads,
                                    const uint32_t* sic_rs, const uint32_t* sic_src,
                                    const uint32_t* e2a_rs, const uint32_t* e2a_src);
 
+/*
+ * oracle_create with biology constants overridden by name (the reference's
+ * Biology fields, src/astrosim_fused.cu:742-781); cfg's fields apply after them,
+ * as in the reference's main.  Returns NULL for an unknown name.
+ */
+oracle_sim* oracle_create_with_biology(const astrosim_config* cfg, int n_threads, const char* const* names,
+                                       const double* values, size_t n);
+
 void oracle_destroy(oracle_sim* s);
 
 /* Advances n_steps time steps (src/astrosim_fused.cu:1042-1102). */

@@ -43,6 +43,9 @@ def lib():
         L.oracle_seq_normals.argtypes = [C.c_uint64, C.c_uint64, C.c_size_t, C.POINTER(C.c_double)]
         L.oracle_create.restype = P
         L.oracle_create.argtypes = [C.POINTER(abi.Config), C.c_int]
+        L.oracle_create_with_biology.restype = P
+        L.oracle_create_with_biology.argtypes = [C.POINTER(abi.Config), C.c_int, C.POINTER(C.c_char_p),
+                                                 C.POINTER(C.c_double), C.c_size_t]
         L.oracle_create_with_csr.restype = P
         L.oracle_create_with_csr.argtypes = [C.POINTER(abi.Config), C.c_int] + [u32p] * 8
         L.oracle_destroy.argtypes = [P]
@@ -88,10 +91,15 @@ def seq_normals(seed, stream, n):
 class OracleSim:
     """One FP64 network on the host, stepped exactly as the reference's time loop."""
 
-    def __init__(self, cfg=None, threads=0, csrs=None, **overrides):
+    def __init__(self, cfg=None, threads=0, csrs=None, biology=None, **overrides):
+        """`biology`: {name: value} overrides of the biology constants (flags as bool)."""
         self.cfg = cfg if cfg is not None else abi.default_config(**overrides)
         L = lib()
-        if csrs is None:
+        if biology:
+            names = (C.c_char_p * len(biology))(*[k.encode() for k in biology])
+            values = (C.c_double * len(biology))(*[float(v) for v in biology.values()])
+            self._h = L.oracle_create_with_biology(C.byref(self.cfg), threads, names, values, len(biology))
+        elif csrs is None:
             self._h = L.oracle_create(C.byref(self.cfg), threads)
         else:
             arrs = []
