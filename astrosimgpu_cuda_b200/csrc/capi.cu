@@ -13,6 +13,7 @@
 #include "../../include/astrosim.h"
 #include "biology.cuh"
 #include "ensemble.cuh"
+#include "shard.cuh"
 #include "reduce.cuh"
 #include "server.cuh"
 #include "sim.cuh"
@@ -423,4 +424,140 @@ int astrosim_biology_value(const char* biology_json, const char* name, double* v
         AS_TRY(astrosim::apply_biology_json(biology_json, b));
         return astrosim::biology_get(b, name, value);
     });
+}
+
+struct astrosim_shard {
+    astrosim::ShardRank r;
+};
+
+struct astrosim_shard_group {
+    astrosim::ShardGroup g;
+};
+
+int astrosim_shard_plan(uint32_t n_total, int rank, int world, uint32_t* neuron_lo, uint32_t* neuron_hi,
+                        uint32_t* astro_lo, uint32_t* astro_hi) {
+    if (world < 1 || rank < 0 || rank >= world || n_total == 0)
+        return fail(ASTROSIM_ERR_INVALID_ARG, "need n_total > 0 and 0 <= rank < world");
+    const astrosim::Sizes sz = astrosim::scaling_law(n_total);
+    const astrosim::ShardPlan p = astrosim::shard_plan(sz.n_neurons, sz.n_astro, rank, world);
+    if (neuron_lo) *neuron_lo = p.n_lo;
+    if (neuron_hi) *neuron_hi = p.n_hi;
+    if (astro_lo) *astro_lo = p.a_lo;
+    if (astro_hi) *astro_hi = p.a_hi;
+    return ASTROSIM_OK;
+}
+
+int astrosim_shard_unique_id(unsigned char id[128]) {
+    if (!id) return fail(ASTROSIM_ERR_INVALID_ARG, "null id");
+    return guarded([&] { return astrosim::nccl_unique_id(id); });
+}
+
+int astrosim_shard_create(const astrosim_config* cfg, const char* biology_json, int rank, int world,
+                          astrosim_shard** out) {
+    if (!cfg || !out) return fail(ASTROSIM_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    if (cfg->struct_size != sizeof(astrosim_config))
+        return fail(ASTROSIM_ERR_INVALID_ARG, "astrosim_config.struct_size mismatch");
+    astrosim_shard* s = nullptr;
+    try {
+        s = new astrosim_shard();
+    } catch (...) {
+        return fail(ASTROSIM_ERR_OUT_OF_MEMORY, "host allocation failed");
+    }
+    const int rc = guarded([&] { return s->r.create(*cfg, biology_json, rank, world); });
+    if (rc != ASTROSIM_OK) {
+        const std::string msg = g_last_error;
+        delete s;
+        g_last_error = msg;
+        return rc;
+    }
+    *out = s;
+    return ASTROSIM_OK;
+}
+
+int astrosim_shard_connect(astrosim_shard* s, const unsigned char id[128]) {
+    if (!s || !id) return fail(ASTROSIM_ERR_INVALID_ARG, "null argument");
+    return guarded([&] { return s->r.connect(id); });
+}
+
+int astrosim_shard_step(astrosim_shard* s, int64_t n_steps) {
+    if (!s) return fail(ASTROSIM_ERR_INVALID_ARG, "null handle");
+    return guarded([&] { return s->r.step(n_steps); });
+}
+
+int astrosim_shard_summary(astrosim_shard* s, astrosim_summary_t* out) {
+    if (!s || !out) return fail(ASTROSIM_ERR_INVALID_ARG, "null argument");
+    return guarded([&] { return s->r.summary(*out); });
+}
+
+int astrosim_shard_get_state(astrosim_shard* s, int which, double* dst, size_t count) {
+    if (!s) return fail(ASTROSIM_ERR_INVALID_ARG, "null handle");
+    return guarded([&] { return s->r.get_state(which, dst, count); });
+}
+
+int astrosim_shard_spike_counts(astrosim_shard* s, int64_t first_step, int64_t n, uint32_t* counts) {
+    if (!s) return fail(ASTROSIM_ERR_INVALID_ARG, "null handle");
+    return guarded([&] {
+        if (!s->r.has_shard()) return astrosim::make_error(ASTROSIM_ERR_STATE, "no shard");
+        return s->r.shard().sim.spike_counts(first_step, n, counts);
+    });
+}
+
+int astrosim_shard_last_step_ms(astrosim_shard* s, double* ms) {
+    if (!s || !ms) return fail(ASTROSIM_ERR_INVALID_ARG, "null argument");
+    *ms = s->r.last_step_ms();
+    return ASTROSIM_OK;
+}
+
+int astrosim_shard_destroy(astrosim_shard* s) {
+    delete s;
+    return ASTROSIM_OK;
+}
+
+int astrosim_shard_group_create(const astrosim_config* cfg, const char* biology_json, int world, const int* devices,
+                                astrosim_shard_group** out) {
+    if (!cfg || !out) return fail(ASTROSIM_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    if (cfg->struct_size != sizeof(astrosim_config))
+        return fail(ASTROSIM_ERR_INVALID_ARG, "astrosim_config.struct_size mismatch");
+    astrosim_shard_group* g = nullptr;
+    try {
+        g = new astrosim_shard_group();
+    } catch (...) {
+        return fail(ASTROSIM_ERR_OUT_OF_MEMORY, "host allocation failed");
+    }
+    const int rc = guarded([&] { return g->g.create(*cfg, biology_json, world, devices); });
+    if (rc != ASTROSIM_OK) {
+        const std::string msg = g_last_error;
+        delete g;
+        g_last_error = msg;
+        return rc;
+    }
+    *out = g;
+    return ASTROSIM_OK;
+}
+
+int astrosim_shard_group_step(astrosim_shard_group* g, int64_t n_steps) {
+    if (!g) return fail(ASTROSIM_ERR_INVALID_ARG, "null handle");
+    return guarded([&] { return g->g.step(n_steps); });
+}
+
+int astrosim_shard_group_summary(astrosim_shard_group* g, astrosim_summary_t* out) {
+    if (!g || !out) return fail(ASTROSIM_ERR_INVALID_ARG, "null argument");
+    return guarded([&] { return g->g.summary(*out); });
+}
+
+int astrosim_shard_group_get_state(astrosim_shard_group* g, int which, double* dst, size_t count) {
+    if (!g) return fail(ASTROSIM_ERR_INVALID_ARG, "null handle");
+    return guarded([&] { return g->g.get_state(which, dst, count); });
+}
+
+int astrosim_shard_group_spike_counts(astrosim_shard_group* g, int64_t first_step, int64_t n, uint32_t* counts) {
+    if (!g) return fail(ASTROSIM_ERR_INVALID_ARG, "null handle");
+    return guarded([&] { return g->g.spike_counts(first_step, n, counts); });
+}
+
+int astrosim_shard_group_destroy(astrosim_shard_group* g) {
+    delete g;
+    return ASTROSIM_OK;
 }

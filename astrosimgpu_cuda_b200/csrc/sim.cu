@@ -464,52 +464,60 @@ __global__ void to_double_kernel(const R* src, double* dst, u64 n) {
 }
 }  // namespace
 
-Status Simulation::get_state(int which, double* dst, size_t count) {
-    if (!dst) return make_error(ASTROSIM_ERR_INVALID_ARG, "null destination");
+Status Simulation::state_location(int which, void** ptr, size_t* elem, u64* count, bool* per_astro) {
     const u64 nN = rc_.n_neurons, nA = rc_.n_astro;
-    const double* dptr = nullptr;
-    const unsigned char* rptr = nullptr;  // real-typed source
-    u64 n = 0;
     const size_t rb = fp32_ ? sizeof(float) : sizeof(double);
-    const unsigned char* g = st_.g_raw.get();
+    unsigned char* g = st_.g_raw.get();
+    void* p = nullptr;
+    size_t e = sizeof(double);
+    bool astro = false;
     switch (which) {
-        case ASTROSIM_STATE_CA: dptr = st_.Ca.get(); n = nA; break;
-        case ASTROSIM_STATE_IP3: dptr = st_.IP3.get(); n = nA; break;
-        case ASTROSIM_STATE_H: rptr = g + 7 * nN * rb; n = nA; break;
-        case ASTROSIM_STATE_V: dptr = st_.V.get(); n = nN; break;
-        case ASTROSIM_STATE_W: dptr = st_.w.get(); n = nN; break;
-        case ASTROSIM_STATE_G_EX: rptr = g; n = nN; break;
-        case ASTROSIM_STATE_DG_EX: rptr = g + 1 * nN * rb; n = nN; break;
-        case ASTROSIM_STATE_G_IN: rptr = g + 2 * nN * rb; n = nN; break;
-        case ASTROSIM_STATE_DG_IN: rptr = g + 3 * nN * rb; n = nN; break;
-        case ASTROSIM_STATE_I_SIC: rptr = g + 4 * nN * rb; n = nN; break;
-        case ASTROSIM_STATE_STP_X: rptr = g + 5 * nN * rb; n = nN; break;
-        case ASTROSIM_STATE_STP_U: rptr = g + 6 * nN * rb; n = nN; break;
-        case ASTROSIM_STATE_STP_T_LAST: dptr = st_.stp_t.get(); n = nN; break;
-        case ASTROSIM_STATE_CA_TOT: dptr = net_.Ca_tot.get(); n = nA; break;
-        case ASTROSIM_STATE_IP3_0: dptr = net_.IP3_0.get(); n = nA; break;
-        case ASTROSIM_STATE_TAU_IP3: dptr = net_.tau_IP3.get(); n = nA; break;
-        case ASTROSIM_STATE_DELTA_IP3: dptr = net_.delta_IP3.get(); n = nA; break;
-        case ASTROSIM_STATE_V_RESET: dptr = net_.V_reset.get(); n = nN; break;
-        case ASTROSIM_STATE_B: dptr = net_.b.get(); n = nN; break;
-        case ASTROSIM_STATE_SIC_FACTOR: rptr = st_.sic_last_raw.get(); n = nA; break;
+        case ASTROSIM_STATE_CA: p = st_.Ca.get(); astro = true; break;
+        case ASTROSIM_STATE_IP3: p = st_.IP3.get(); astro = true; break;
+        case ASTROSIM_STATE_H: p = g + 7 * nN * rb; e = rb; astro = true; break;
+        case ASTROSIM_STATE_V: p = st_.V.get(); break;
+        case ASTROSIM_STATE_W: p = st_.w.get(); break;
+        case ASTROSIM_STATE_G_EX: p = g; e = rb; break;
+        case ASTROSIM_STATE_DG_EX: p = g + 1 * nN * rb; e = rb; break;
+        case ASTROSIM_STATE_G_IN: p = g + 2 * nN * rb; e = rb; break;
+        case ASTROSIM_STATE_DG_IN: p = g + 3 * nN * rb; e = rb; break;
+        case ASTROSIM_STATE_I_SIC: p = g + 4 * nN * rb; e = rb; break;
+        case ASTROSIM_STATE_STP_X: p = g + 5 * nN * rb; e = rb; break;
+        case ASTROSIM_STATE_STP_U: p = g + 6 * nN * rb; e = rb; break;
+        case ASTROSIM_STATE_STP_T_LAST: p = st_.stp_t.get(); break;
+        case ASTROSIM_STATE_CA_TOT: p = net_.Ca_tot.get(); astro = true; break;
+        case ASTROSIM_STATE_IP3_0: p = net_.IP3_0.get(); astro = true; break;
+        case ASTROSIM_STATE_TAU_IP3: p = net_.tau_IP3.get(); astro = true; break;
+        case ASTROSIM_STATE_DELTA_IP3: p = net_.delta_IP3.get(); astro = true; break;
+        case ASTROSIM_STATE_V_RESET: p = net_.V_reset.get(); break;
+        case ASTROSIM_STATE_B: p = net_.b.get(); break;
+        case ASTROSIM_STATE_SIC_FACTOR: p = st_.sic_last_raw.get(); e = rb; astro = true; break;
         default: return make_error(ASTROSIM_ERR_INVALID_ARG, "unknown state array %d", which);
     }
+    *ptr = p;
+    *elem = e;
+    *count = astro ? nA : nN;
+    if (per_astro) *per_astro = astro;
+    return Status::Ok();
+}
+
+Status Simulation::get_state(int which, double* dst, size_t count) {
+    if (!dst) return make_error(ASTROSIM_ERR_INVALID_ARG, "null destination");
+    void* src = nullptr;
+    size_t elem = 0;
+    u64 n = 0;
+    AS_TRY(state_location(which, &src, &elem, &n, nullptr));
     if (count < n) return make_error(ASTROSIM_ERR_INVALID_ARG, "state array needs %llu elements",
                                      static_cast<unsigned long long>(n));
     AS_CUDA(cudaSetDevice(device_));
-    if (dptr) {
-        AS_CUDA(cudaMemcpyAsync(dst, dptr, n * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    if (elem == sizeof(double)) {  // double arrays, and `real` arrays of the FP64 path
+        AS_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToHost, stream_));
     } else {
         AllocStream alloc_scope(stream_);
         DevBuf<double> tmp;
         AS_TRY(tmp.alloc(n));
-        if (fp32_)
-            to_double_kernel<float><<<ceil_div(n, 256), 256, 0, stream_>>>(reinterpret_cast<const float*>(rptr),
-                                                                          tmp.get(), n);
-        else
-            to_double_kernel<double><<<ceil_div(n, 256), 256, 0, stream_>>>(reinterpret_cast<const double*>(rptr),
-                                                                           tmp.get(), n);
+        to_double_kernel<float><<<ceil_div(n, 256), 256, 0, stream_>>>(reinterpret_cast<const float*>(src),
+                                                                      tmp.get(), n);
         AS_CUDA(cudaGetLastError());
         AS_CUDA(cudaMemcpyAsync(dst, tmp.get(), n * sizeof(double), cudaMemcpyDeviceToHost, stream_));
         AS_CUDA(cudaStreamSynchronize(stream_));

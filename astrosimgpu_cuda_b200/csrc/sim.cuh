@@ -77,6 +77,9 @@ public:
     Status spike_counts(i64 first, i64 n, u32* dst);
     Status raster(u32* dst, size_t words);
     Status get_state(int which, double* dst, size_t count);
+    // Device location of a STATE_* array: base, element size (8, or 4 for `real` arrays
+    // in the FP32 form), length, and whether it has one entry per astrocyte.
+    Status state_location(int which, void** ptr, size_t* elem, u64* count, bool* per_astro);
     Status get_csr(int which, u32* rs, size_t rs_cap, u32* src, size_t src_cap, u32* n_targets, u64* n_edges);
     Status dump_edges(const char* path);
     Status last_step_ms(double* ms);

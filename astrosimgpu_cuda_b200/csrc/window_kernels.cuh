@@ -297,9 +297,12 @@ __device__ __forceinline__ void window_cells(const RunConsts& rc, const StepPtrs
 // After window `buf` completes: deliver its spikes into the inboxes of the next
 // window (buffer buf ^ 1), or switch the next window to pull when it was busy.
 // Blocks 0 .. n_blk-1 share the spike list.
+// Targets outside [t_lo, t_hi) (neurons) and [a_lo, a_hi) (astrocytes) are skipped:
+// a rank of a sharded network delivers only into the cells it owns.
 template <typename R>
 __device__ __forceinline__ void push_cells(const WinPtrs<R>& w, u32 n_exc, u32 n_inh, u64 n_neurons, u64 n_astro,
-                                           int buf, u32 blk, u32 n_blk) {
+                                           int buf, u32 blk, u32 n_blk, u32 t_lo = 0, u32 t_hi = 0xFFFFFFFFu,
+                                           u32 a_lo = 0, u32 a_hi = 0xFFFFFFFFu) {
     const int nxt = buf ^ 1;
     const u32 n = w.spk_count[buf];
     const bool busy = n > w.push_limit;
@@ -319,12 +322,14 @@ __device__ __forceinline__ void push_cells(const WinPtrs<R>& w, u32 n_exc, u32 n
         if (j < n_exc) {
             for (u32 k = w.fe_rs[j] + lane; k < w.fe_rs[j + 1]; k += 32) {
                 const u32 t = w.fe_dst[k];
+                if (t < t_lo || t >= t_hi) continue;
                 const u64 sb = static_cast<u64>(nxt) * n_neurons + t;
                 const u32 slot = atomicAdd(&w.nin_cnt[sb], 1u);
                 if (slot < kInboxSlots) w.nin_ent[sb * kInboxSlots + slot] = Deposit<R>{j, st, v};
             }
             for (u32 k = w.fa_rs[j] + lane; k < w.fa_rs[j + 1]; k += 32) {
                 const u32 a = w.fa_astro[k];
+                if (a < a_lo || a >= a_hi) continue;
                 const u64 sb = static_cast<u64>(nxt) * n_astro + a;
                 const u32 slot = atomicAdd(&w.ain_cnt[sb], 1u);
                 if (slot < kInboxSlots) w.ain_ent[sb * kInboxSlots + slot] = Deposit<R>{w.fa_pos[k], st, v};
@@ -335,6 +340,7 @@ __device__ __forceinline__ void push_cells(const WinPtrs<R>& w, u32 n_exc, u32 n
         if (j < n_inh) {
             for (u32 k = w.fi_rs[j] + lane; k < w.fi_rs[j + 1]; k += 32) {
                 const u32 t = w.fi_dst[k];
+                if (t < t_lo || t >= t_hi) continue;
                 const u64 sb = static_cast<u64>(nxt) * n_neurons + t;
                 const u32 slot = atomicAdd(&w.nin_cnt[sb], 1u);
                 if (slot < kInboxSlots) w.nin_ent[sb * kInboxSlots + slot] = Deposit<R>{j, st | (1u << 8), v};

@@ -377,6 +377,53 @@ typedef struct astrosim_astro_totals {
 int astrosim_astro_totals_noalloc(const double* ca, const unsigned char* engaged, uint32_t n_astro, double sic_th,
                                   astrosim_astro_totals* out, void* stream);
 
+/* ------------------------------------------------------------------ one network on several GPUs
+ * A network split across `world` ranks (SURVEY's multi-GPU form; the reference
+ * runs on one GPU).  Every rank builds the whole network and owns contiguous
+ * ranges of neurons and astrocytes (128-cell blocks, balanced); per 1 ms window
+ * it advances its own cells, then the ranks all-gather the window's spikes and the
+ * SIC factors of their active astrocytes, and each rank delivers every spike into
+ * its own cells.  Results (spike counts, raster, every state array, the summary)
+ * are bit-identical to the single-GPU run.  Stepping is in whole windows.  The
+ * windowed engine is required (equal delays of 2-16 steps).
+ */
+
+/* Owned ranges of rank `rank` of `world` for n_total (host only, no device). */
+int astrosim_shard_plan(uint32_t n_total, int rank, int world, uint32_t* neuron_lo, uint32_t* neuron_hi,
+                        uint32_t* astro_lo, uint32_t* astro_hi);
+
+/* One rank per process over NCCL (libnccl.so.2, loaded when first used).
+   astrosim_shard_create builds this rank's network without communicating; cfg (and
+   biology_json) must be identical on every rank except cfg.device, the rank's GPU.
+   Once every rank has created its part (the caller checks that, e.g. with
+   torch.distributed, so that no rank waits for one that failed), rank 0 makes the
+   128-byte id with astrosim_shard_unique_id, the caller hands the same bytes to
+   every rank, and each calls astrosim_shard_connect (collective).  step, summary
+   and get_state are collective: every rank calls them in the same order. */
+typedef struct astrosim_shard astrosim_shard;
+int astrosim_shard_unique_id(unsigned char id[128]);
+int astrosim_shard_create(const astrosim_config* cfg, const char* biology_json, int rank, int world,
+                          astrosim_shard** out);
+int astrosim_shard_connect(astrosim_shard* s, const unsigned char id[128]);
+int astrosim_shard_step(astrosim_shard* s, int64_t n_steps);
+int astrosim_shard_summary(astrosim_shard* s, astrosim_summary_t* out);
+int astrosim_shard_get_state(astrosim_shard* s, int which, double* dst, size_t count);
+int astrosim_shard_spike_counts(astrosim_shard* s, int64_t first_step, int64_t n, uint32_t* counts);
+/* Device time of this rank's last astrosim_shard_step, ms (take the max over ranks). */
+int astrosim_shard_last_step_ms(astrosim_shard* s, double* ms);
+int astrosim_shard_destroy(astrosim_shard* s);
+
+/* All ranks in this process: rank r runs on devices[r] (NULL: every rank on
+   cfg.device; ranks that share a device run one after another).  Same results. */
+typedef struct astrosim_shard_group astrosim_shard_group;
+int astrosim_shard_group_create(const astrosim_config* cfg, const char* biology_json, int world, const int* devices,
+                                astrosim_shard_group** out);
+int astrosim_shard_group_step(astrosim_shard_group* g, int64_t n_steps);
+int astrosim_shard_group_summary(astrosim_shard_group* g, astrosim_summary_t* out);
+int astrosim_shard_group_get_state(astrosim_shard_group* g, int which, double* dst, size_t count);
+int astrosim_shard_group_spike_counts(astrosim_shard_group* g, int64_t first_step, int64_t n, uint32_t* counts);
+int astrosim_shard_group_destroy(astrosim_shard_group* g);
+
 /*
  * Device arithmetic self-check: the FP64 right-hand sides divide by the model's
  * constants (C_m, tau_w, Delta_T, ratio_ER_cyt and each astrocyte's tau_IP3) with a
