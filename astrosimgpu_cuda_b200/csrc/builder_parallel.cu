@@ -475,6 +475,7 @@ Status section_orbit(const SectionPlan& P, Sec s, u64 start, DevBuf<int>& err, D
     u32 chunk_len = P.chunk_len, delta = P.delta;
     double slack = 1.04;
     int K = 32;
+    PhaseClock pc(st);
     for (int attempt = 0; attempt < 8; ++attempt) {
         AS_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(int), st));
         const u64 margin = P.autapse_shifts_stream ? static_cast<u64>(K) + 16 : 0;
@@ -505,6 +506,7 @@ Status section_orbit(const SectionPlan& P, Sec s, u64 start, DevBuf<int>& err, D
         u32 hend = 0;
         AS_TRY(read_err(err, &herr, st));
         AS_TRY(to_host(&hend, endg.get(), 1, st));
+        pc.mark("  chunk tables + composition");
         if (herr & kErrHash) { chunk_len /= 2; continue; }
         if (herr & kErrDelta) {
             if (delta >= kMaxDelta) return make_error(ASTROSIM_ERR_UNSUPPORTED, "%s: a pre longer than %u draws", P.name, kMaxDelta);
@@ -542,6 +544,7 @@ Status section_orbit(const SectionPlan& P, Sec s, u64 start, DevBuf<int>& err, D
             continue;
         }
         if (herr) return make_error(ASTROSIM_ERR_CUDA, "%s orbit materialisation failed (flags %d)", P.name, herr);
+        pc.mark("  chunk entries + orbit");
 
         if (!P.autapse_shifts_stream) {
             orbit = std::move(forbit);
@@ -571,6 +574,7 @@ Status section_orbit(const SectionPlan& P, Sec s, u64 start, DevBuf<int>& err, D
         std::sort(hh.begin(), hh.end(), [](const Hazard& a, const Hazard& b) {
             return a.r != b.r ? a.r < b.r : a.d < b.d;
         });
+        pc.mark("  autapse hazards");
         // speculative exact walks from every hazard
         const u32 max_explicit = 8192;
         DevBuf<Hazard> hz_sorted;
@@ -589,6 +593,7 @@ Status section_orbit(const SectionPlan& P, Sec s, u64 start, DevBuf<int>& err, D
             AS_TRY(read_err(err, &herr, st));
             if (herr) return make_error(ASTROSIM_ERR_UNSUPPORTED, "%s: re-merge walks failed (flags %d)", P.name, herr);
         }
+        pc.mark("  re-merge walks");
         // replay the hazards in order with the running shift (true index - table index)
         struct Piece { bool expl; u64 t_start, src, len; };
         std::vector<Piece> pieces;

@@ -336,6 +336,7 @@ Status draw_cell_parameters(const Sizes& sz, u64 seed, const Biology& bio, Netwo
     pa.n_units = 4ull * nA;
     pa.k_start = 0;
 
+    PhaseClock pc(st);
     // The normals k map to uniforms 2*(k/2), 2*(k/2)+1 only while no pair's first
     // uniform is exactly zero (the reference would redraw it).  Check the range used.
     {
@@ -353,9 +354,11 @@ Status draw_cell_parameters(const Sizes& sz, u64 seed, const Biology& bio, Netwo
                               static_cast<unsigned long long>(seed));
     }
 
+    pc.mark("  zero-draw scan");
     double* adst[4] = {net.Ca_tot.get(), net.IP3_0.get(), net.tau_IP3.get(), net.delta_IP3.get()};
     u64 k = 0;
     AS_TRY(run_phase(pa, seed, adst, nA, &k, st));
+    pc.mark("  astrocyte parameters");
 
     // src/astrosim_fused.cu:927-933: V_reset then b per neuron; exc then inh means
     for (int pop = 0; pop < 2; ++pop) {
@@ -371,6 +374,7 @@ Status draw_cell_parameters(const Sizes& sz, u64 seed, const Biology& bio, Netwo
         pn.k_start = k;
         double* ndst[2] = {net.V_reset.get() + first, net.b.get() + first};
         AS_TRY(run_phase(pn, seed, ndst, n_cells, &k, st));
+        pc.mark(exc ? "  excitatory parameters" : "  inhibitory parameters");
     }
     return Status::Ok();
 }
