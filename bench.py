@@ -41,6 +41,9 @@ PRE_MS, SIM_MS = 100.0, 500.0
 # N_total = 1e6 steady state (profiles/window_kernel_*_n1e6_steady.md); traffic
 # grows with the cell count, so a launch at N carries about N / 1e6 times this.
 PROFILED_WINDOW_TRAFFIC_1E6 = {"fp32": 176.8e6, "fp64": 409.9e6}
+# Fraction of issue slots busy in the same captures: the window kernel is bound by
+# instruction issue, not by HBM, which is why roofline.frac against HBM stays low.
+PROFILED_ISSUE_ACTIVE = {"fp32": 0.728, "fp64": 0.559}
 
 
 def peaks():
@@ -372,6 +375,28 @@ def ours_sequential(cfgs, sample):
     return sum(times) / len(times)
 
 
+def run_seed_sweep(args, local):
+    """Config C3's seeds 1-3 at N=1e7: FP32 against FP64 on the same network (mean rate, SIC fraction)."""
+    import astrosimgpu_cuda_b200 as asg
+
+    out = []
+    for seed in (1, 2, 3):
+        row = {"seed": seed}
+        for prec in ("fp32", "fp64"):
+            with asg.Simulation(n_total=N_TOTAL, seed=seed, pre_ms=PRE_MS, sim_ms=SIM_MS, precision=prec,
+                                device=local) as sim:
+                sim.step(sim.summary()["total_steps"])
+                sm = sim.summary()
+            row[prec] = {"mean_rate_hz": sm["mean_rate_hz"], "sic_fraction": sm["active_astro"] / sm["n_astro"],
+                         "engaged_fraction": sm["engaged_astro"] / sm["n_astro"], "mean_ca": sm["mean_ca"],
+                         "spikes_measured": sm["spikes_measured"]}
+        a, b = row["fp32"], row["fp64"]
+        row["fp32_rate_rel_err"] = abs(a["mean_rate_hz"] - b["mean_rate_hz"]) / max(b["mean_rate_hz"], 1e-300)
+        row["fp32_sic_fraction_abs_err"] = abs(a["sic_fraction"] - b["sic_fraction"])
+        out.append(row)
+    return out
+
+
 def run_ensemble(args):
     """256 networks, N_total log-uniform in [500, 50000], 2000 ms each, FP32 (the batched configuration)."""
     import numpy as np
@@ -502,6 +527,7 @@ def main():
     ap.add_argument("--n", type=int, default=N_TOTAL, help="network size (the benchmark is N=1e7)")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-seed-sweep", action="store_true", help="skip the seeds 1-3 FP32 vs FP64 comparison")
     ap.add_argument("--ens-networks", type=int, default=256)
     ap.add_argument("--serve-requests", type=int, default=2000)
     ap.add_argument("--serve-rates", default="5,20,50,200", help="comma-separated arrival rates (req/s)")
@@ -559,6 +585,8 @@ def main():
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one window_kernel launch "
                                        "at N_total=1e6 (profiles/), scaled by N_total / 1e6",
                      "peak_source": peak_kind,
+                     "issue_slots_busy": PROFILED_ISSUE_ACTIVE["fp32" if "fp32" in res else "fp64"],
+                     "issue_source": "ncu smsp__issue_active of the same window_kernel capture (profiles/)",
                      "kernel": "window_kernel<float> (one launch = one 10-step window); its push_kernel, 1.5 % of "
                                "the window time in the launch list, is inside the timed duration",
                      "algorithmic_bytes_per_launch": f32["bytes"] * 10,
@@ -578,6 +606,8 @@ def main():
                         "syn_events_per_s": f64["e_visit"] * ws * args.steps / (f64["ms"] * 1e-3),
                         "clocks": f64["clocks"]}
         line["fp32_over_fp64"] = f64["ms"] / f32["ms"]
+    if args.precision == "both" and ws == 1 and args.n == 10_000_000 and not args.no_seed_sweep:
+        line["fp32_vs_fp64_seeds"] = run_seed_sweep(args, local)
     if not args.no_ensemble and ws == 1 and args.n == 10_000_000:
         line["ensemble"] = run_ensemble(args)
     if not args.no_serving and ws == 1 and args.n == 10_000_000:
