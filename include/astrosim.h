@@ -378,7 +378,7 @@ int astrosim_astro_totals_noalloc(const double* ca, const unsigned char* engaged
                                   astrosim_astro_totals* out, void* stream);
 
 /* ------------------------------------------------------------------ one network on several GPUs
- * A network split across `world` ranks (SURVEY's multi-GPU form; the reference
+ * A network split across `world` ranks (the reference
  * runs on one GPU).  Every rank builds the whole network and owns contiguous
  * ranges of neurons and astrocytes (128-cell blocks, balanced); per 1 ms window
  * it advances its own cells, then the ranks all-gather the window's spikes and the

@@ -99,7 +99,7 @@ def test_fp64_raster_identical_first_200ms(n_total, seed):
 
 
 def test_fp64_full_config0_summary():
-    """N=500, seed 1, 1000 ms pre-run + 5000 ms recorded."""
+    """The reference's small CPU-sized case: N=500, seed 1, 1000 ms pre-run + 5000 ms recorded."""
     o = oracle.OracleSim(n_total=500, seed=1)
     with asg.Simulation(n_total=500, seed=1) as sim:
         total = sim.summary()["total_steps"]
