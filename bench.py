@@ -418,15 +418,16 @@ def run_ensemble(args):
         rates = [ens.summary(i)["mean_rate_hz"] for i in range(n)]
     wall = time.perf_counter() - t0
     sample = [int(x) for x in rng.choice(n, size=min(n, args.baseline_sample), replace=False)]
-    ours = ours_sequential(cfgs, sample)
-    ref = reference_sequential(cfgs, sample)
+    ours = ours_sequential(cfgs, sample) if sample else None
+    ref = reference_sequential(cfgs, sample) if sample else None
     out = {"networks": n, "n_total_sum": int(sum(c.n_total for c in cfgs)), "sim_ms": 2000.0, "dtype": "f32",
            "sims_per_s": n / wall, "sims_per_s_stepping_only": n / (step_ms * 1e-3),
            "build_s": build_s, "stepping_s": step_ms * 1e-3, "wall_s": wall,
-           "mean_rate_hz": float(np.mean(rates)),
-           "plain_path_sequential_sims_per_s": 1.0 / ours,
-           "baseline_sample": f"{len(sample)} of the {n} networks, run one after another",
-           "speedup_vs_plain_path_sequential": (n / wall) * ours}
+           "mean_rate_hz": float(np.mean(rates))}
+    if ours:
+        out.update({"plain_path_sequential_sims_per_s": 1.0 / ours,
+                    "baseline_sample": f"{len(sample)} of the {n} networks, run one after another",
+                    "speedup_vs_plain_path_sequential": (n / wall) * ours})
     if ref:
         out["reference_sequential_sims_per_s"] = 1.0 / ref
         out["speedup_vs_reference_sequential"] = (n / wall) * ref
@@ -502,7 +503,9 @@ def serving_sweep(args):
                                       "200-2000 ms, drive within +-20 %, seeds random",
            "requests_per_rate": f"min({args.serve_requests}, ceil(rate x {args.serve_window:g} s))",
            "rates": [run_serving(args, r) for r in rates]}
-    cfgs = serving_configs(max(args.baseline_sample, 1), 99)
+    if args.baseline_sample <= 0:
+        return out
+    cfgs = serving_configs(args.baseline_sample, 99)
     sample = list(range(len(cfgs)))
     ours = ours_sequential(cfgs, sample)
     out["plain_path_sequential_sims_per_s"] = 1.0 / ours
@@ -528,6 +531,8 @@ def main():
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-seed-sweep", action="store_true", help="skip the seeds 1-3 FP32 vs FP64 comparison")
+    ap.add_argument("--leg", choices=("ensemble", "serving"), default=None,
+                    help="run only the batched ensemble or the serving sweep (profiling captures)")
     ap.add_argument("--ens-networks", type=int, default=256)
     ap.add_argument("--serve-requests", type=int, default=2000)
     ap.add_argument("--serve-rates", default="5,20,50,200", help="comma-separated arrival rates (req/s)")
@@ -550,6 +555,12 @@ def main():
         line = run_reference(args, ws, rank)
         if rank == 0:
             print(json.dumps(line), flush=True)
+        return
+
+    if args.leg:  # one form alone, for profiling captures
+        if ws == 1:
+            leg = run_ensemble(args) if args.leg == "ensemble" else serving_sweep(args)
+            print(json.dumps({"leg": args.leg, args.leg: leg}), flush=True)
         return
 
     if args.shard:
