@@ -141,10 +141,12 @@ Status Ensemble::create(const astrosim_config* cfgs, u32 n, const char* const* b
     nets_.resize(n);
     std::vector<Status> st(n);
     std::atomic<u32> next{0};
-    // Builds overlap on the GPU but each waits on the host between its kernels; past
-    // about half the host cores the waiting threads contend for CPU (measured on a
-    // 16-core host: 8 threads build 64 networks 2.5x faster than 16 at N = 20000).
-    const u32 workers = std::min<u32>(n, std::max(1u, std::min(8u, std::thread::hardware_concurrency() / 2)));
+    // Builds overlap on the GPU but each waits on the host between its kernels, so
+    // the threads contend for CPU past about three quarters of the host cores
+    // (measured on a 16-core host: 12 threads build 62-71 networks/s at N = 2e3-2e4,
+    // 8 threads 59-76, 16 threads 51-80).
+    const u32 workers =
+        std::min<u32>(n, std::max(1u, std::min(12u, std::thread::hardware_concurrency() * 3 / 4)));
     auto work = [&] {
         for (u32 i = next++; i < n; i = next++) {
             auto s = std::make_unique<Simulation>();

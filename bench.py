@@ -462,7 +462,7 @@ def run_serving(args, rate):
     submit_t = np.zeros(n)
     ids = []
     deadline = args.serve_timeout
-    with asg.Server(precision="fp32", builders=8) as srv:
+    with asg.Server(precision="fp32", builders=12) as srv:
         t0 = time.perf_counter()
         i = 0
         while True:
