@@ -69,7 +69,7 @@ struct AllocStream {
     AllocStream& operator=(const AllocStream&) = delete;
 };
 
-constexpr size_t kPoolMaxBytes = size_t(64) << 20;
+constexpr size_t kPoolMaxBytes = size_t(256) << 20;
 
 // Owning device allocation, movable, never copied.  It is freed on the stream it was
 // allocated on; the owner keeps that stream alive until its buffers are released.
@@ -102,8 +102,10 @@ public:
         void* p = nullptr;
         // Buffers of kPoolMaxBytes or more come straight from cudaMalloc: growing the
         // stream-ordered pool by gigabytes the first time costs seconds (measured:
-        // a first N = 1e7 build took 4.0 s from the pool, 1.4 s without it), and a
-        // few large frees that synchronize the device are harmless.
+        // a first N = 1e7 build took 4.0 s from the pool, 0.6 s without it), and the
+        // few multi-gigabyte frees of a large build, which synchronize the device,
+        // are harmless.  Everything a network of up to a few 1e5 cells allocates
+        // stays stream-ordered, so concurrent builds never wait for each other.
         st_ = n * sizeof(T) < kPoolMaxBytes ? alloc_stream() : nullptr;
         cudaError_t e = st_ ? cudaMallocAsync(&p, n * sizeof(T), st_) : cudaMalloc(&p, n * sizeof(T));
         if (e != cudaSuccess) {
