@@ -6,8 +6,11 @@
 #include <cstdarg>
 #include <cstdint>
 #include <cstdio>
+#include <mutex>
 #include <string>
 #include <utility>
+#include <cstddef>
+#include <vector>
 
 #include "../../include/astrosim.h"
 
@@ -139,13 +142,53 @@ private:
     cudaStream_t st_ = nullptr;
 };
 
-// Keeps freed stream-ordered memory in the device pool (up to `bytes`) for reuse.
+// Keeps freed stream-ordered memory in the device pool (up to `bytes`) for reuse;
+// set once per device (the first call wins).
 inline void keep_pool_memory(int device, unsigned long long bytes) {
-    cudaMemPool_t pool = nullptr;
-    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess && pool) {
-        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &bytes);
+    static std::once_flag once[64];
+    if (device < 0 || device >= 64) return;
+    std::call_once(once[device], [&] {
+        cudaMemPool_t pool = nullptr;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess && pool)
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &bytes);
+        cudaGetLastError();
+    });
+}
+
+// Streams handed from one simulation to the next: making and destroying a stream per
+// network is driver work that serialises concurrent builds.  A stream goes back idle
+// (its owner synchronises it first); the pool holds at most the peak number of
+// simulations alive at once and lives until the process exits.
+struct StreamPool {
+    std::mutex mu;
+    std::vector<std::pair<int, cudaStream_t>> idle;  // (device, stream)
+};
+
+inline StreamPool& stream_pool() {
+    static StreamPool* p = new StreamPool();  // never destroyed: streams outlive static destruction order
+    return *p;
+}
+
+// An idle non-blocking stream on `device` (the current device).
+inline cudaError_t take_stream(int device, cudaStream_t* out) {
+    {
+        StreamPool& p = stream_pool();
+        std::lock_guard<std::mutex> lock(p.mu);
+        for (size_t i = 0; i < p.idle.size(); ++i)
+            if (p.idle[i].first == device) {
+                *out = p.idle[i].second;
+                p.idle.erase(p.idle.begin() + static_cast<std::ptrdiff_t>(i));
+                return cudaSuccess;
+            }
     }
-    cudaGetLastError();
+    return cudaStreamCreateWithFlags(out, cudaStreamNonBlocking);
+}
+
+// Returns a stream with no work pending to the pool.
+inline void give_stream(int device, cudaStream_t s) {
+    StreamPool& p = stream_pool();
+    std::lock_guard<std::mutex> lock(p.mu);
+    p.idle.emplace_back(device, s);
 }
 
 inline unsigned ceil_div(uint64_t a, uint64_t b) { return static_cast<unsigned>((a + b - 1) / b); }

@@ -120,8 +120,8 @@ Simulation::~Simulation() {
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
     if (stream_) {
-        cudaStreamSynchronize(stream_);
-        cudaStreamDestroy(stream_);
+        if (cudaStreamSynchronize(stream_) == cudaSuccess) give_stream(device_, stream_);
+        else cudaStreamDestroy(stream_);
     }
 }
 
@@ -148,9 +148,7 @@ Status Simulation::create(const astrosim_config& cfg, const char* biology_json) 
         return make_error(ASTROSIM_ERR_INVALID_ARG, "device %d out of range (%d visible)", cfg.device, ndev);
     device_ = cfg.device;
     AS_CUDA(cudaSetDevice(device_));
-    AS_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
-    AS_CUDA(cudaEventCreate(&ev0_));
-    AS_CUDA(cudaEventCreate(&ev1_));
+    AS_CUDA(take_stream(device_, &stream_));
     keep_pool_memory(device_, 8ull << 30);
     AllocStream alloc_scope(stream_);
 
@@ -317,6 +315,9 @@ Status Simulation::step(i64 n) {
     AS_CUDA(cudaSetDevice(device_));
     AS_TRY(ensure_counts(steps_done_ + n));
     const auto t0 = std::chrono::steady_clock::now();
+    // timing events are made on the first step: networks stepped by a batch never need them
+    if (!ev0_) AS_CUDA(cudaEventCreate(&ev0_));
+    if (!ev1_) AS_CUDA(cudaEventCreate(&ev1_));
     AS_CUDA(cudaEventRecord(ev0_, stream_));
     AS_TRY(launch_steps(steps_done_, n));
     AS_CUDA(cudaEventRecord(ev1_, stream_));

@@ -132,8 +132,6 @@ Status window_setup(const RunConsts& rc, Network& net, bool fp32, WindowState& w
     AS_TRY(ws.sic_win.alloc_zero(2 * nA * ws.W * rb, st));
     AS_TRY(ws.astro_active.alloc_zero(2 * ((nA + 31) / 32), st));
     AS_TRY(ws.mode.alloc_zero(2, st));
-    AS_CUDA(cudaEventCreate(&ws.tune_ev[0]));
-    AS_CUDA(cudaEventCreate(&ws.tune_ev[1]));
     AS_CUDA(cudaStreamSynchronize(st));
     return Status::Ok();
 }
@@ -200,6 +198,10 @@ Status launch_impl(const RunConsts& rc, StateBuffers& sb, Network& net, WindowSt
         const int buf = static_cast<int>(k & 1);
         const bool tuning = ws.variant < 0 && s0 == 0 && s1 == W;
         const int v = ws.variant >= 0 ? ws.variant : (tuning ? ws.tune_step % kNumVariants : 0);
+        if (tuning && !ws.tune_ev[0]) {  // made on the first tuned window only
+            AS_CUDA(cudaEventCreate(&ws.tune_ev[0]));
+            AS_CUDA(cudaEventCreate(&ws.tune_ev[1]));
+        }
         if (tuning) AS_CUDA(cudaEventRecord(ws.tune_ev[0], st));
         launch_window<R>(v, astro_blocks + neuron_blocks, st, rc, p, w, k * W, s0, s1, buf, mark, astro_blocks);
         AS_CUDA(cudaGetLastError());
