@@ -8,6 +8,7 @@ short configurations and parses the lines the reference prints at the end of a
 run (src/astrosim_fused.cu:1131-1141).  Needs a CUDA device; writes JSON.
 
 Usage:  python tests/golden/make_reference_dynamics_golden.py --out reference_dynamics.json
+        (--min-n / --max-n select cases; --merge FILE keeps FILE's other records)
 """
 import argparse
 import json
@@ -25,6 +26,7 @@ CASES = [("fp64", 500, 1, 0, t) for t in (1, 5, 10, 20, 50, 100, 200, 500)] + [
     ("fp64", 5000, 2, 0, 100),
     ("fp64", 2000, 3, 50, 150),
     ("fp64", 1000000, 7, 200, 1000),
+    ("fp64", 10000000, 1, 100, 500),
     ("fp32", 500, 1, 1000, 5000),
     ("fp32", 1000000, 7, 200, 1000),
 ]
@@ -52,15 +54,19 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", required=True)
     ap.add_argument("--max-n", type=int, default=10**7)
+    ap.add_argument("--min-n", type=int, default=0)
+    ap.add_argument("--merge", default=None, help="existing golden file: keep its other records")
     args = ap.parse_args()
-    res = []
+    res = json.load(open(args.merge)) if args.merge else []
     for prec, n, seed, pre, sim in CASES:
-        if n > args.max_n:
+        if n > args.max_n or n < args.min_n:
             continue
         cmd = [BIN[prec], "--n", str(n), "--seed", str(seed), "--pre-ms", str(pre), "--sim-ms", str(sim)]
         r = subprocess.run(cmd, capture_output=True, text=True, timeout=1800)
         rec = {"precision": prec, "n_total": n, "seed": seed, "pre_ms": pre, "sim_ms": sim,
                "returncode": r.returncode, **parse(r.stdout)}
+        key = (prec, n, seed, pre, sim)
+        res = [x for x in res if (x["precision"], x["n_total"], x["seed"], x["pre_ms"], x["sim_ms"]) != key]
         res.append(rec)
         print(json.dumps(rec), flush=True)
     with open(args.out, "w") as f:
