@@ -37,10 +37,12 @@ DT = 0.1
 PRE_MS, SIM_MS = 100.0, 500.0
 
 
-# DRAM bytes (read + write) of one window_kernel launch measured by ncu on the
-# N_total = 1e6 steady state (profiles/window_kernel_*_n1e6_steady.md); traffic
-# grows with the cell count, so a launch at N carries about N / 1e6 times this.
-PROFILED_WINDOW_TRAFFIC_1E6 = {"fp32": 176.8e6, "fp64": 409.9e6}
+# DRAM bytes (read + write) of one window_kernel launch measured by ncu
+# (profiles/): FP32 on the full N_total = 1e7 workload in the timed region (one
+# pass, nothing replayed), FP64 on the N_total = 1e6 steady state; traffic grows
+# with the cell count, so a launch at N carries about N / N_measured times this.
+PROFILED_WINDOW_TRAFFIC = {"fp32": (10_000_000, 2.016e9, "ncu at N_total=1e7, timed region"),
+                           "fp64": (1_000_000, 409.9e6, "ncu at N_total=1e6 steady state, scaled")}
 # Fraction of issue slots busy in the same captures: the window kernel is bound by
 # instruction issue, not by HBM, which is why roofline.frac against HBM stays low.
 PROFILED_ISSUE_ACTIVE = {"fp32": 0.728, "fp64": 0.559}
@@ -592,9 +594,11 @@ def main():
                    "l2": "no flush: per-step working set (CSR 5.3 GB + state) is far larger than the 126 MB L2"},
         "syn_events_per_s": f32["e_visit"] * value,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": PROFILED_WINDOW_TRAFFIC_1E6["fp32" if "fp32" in res else "fp64"] * N_TOTAL / 1e6,
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one window_kernel launch "
-                                       "at N_total=1e6 (profiles/), scaled by N_total / 1e6",
+                     "traffic": PROFILED_WINDOW_TRAFFIC["fp32" if "fp32" in res else "fp64"][1] * N_TOTAL /
+                                PROFILED_WINDOW_TRAFFIC["fp32" if "fp32" in res else "fp64"][0],
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one window_kernel launch, "
+                                       + PROFILED_WINDOW_TRAFFIC["fp32" if "fp32" in res else "fp64"][2]
+                                       + " (profiles/)",
                      "peak_source": peak_kind,
                      "issue_slots_busy": PROFILED_ISSUE_ACTIVE["fp32" if "fp32" in res else "fp64"],
                      "issue_source": "ncu smsp__issue_active of the same window_kernel capture (profiles/)",
