@@ -75,10 +75,12 @@ def lib():
     L.astrosim_ensemble_spike_counts.argtypes = [E, C.c_uint32, C.c_int64, C.c_int64, u32p]
     L.astrosim_ensemble_last_step_ms.argtypes = [E, C.POINTER(C.c_double)]
     L.astrosim_ensemble_build_seconds.argtypes = [E, C.POINTER(C.c_double)]
+    L.astrosim_ensemble_shared_constants.argtypes = [E, C.POINTER(C.c_int)]
     L.astrosim_ensemble_destroy.argtypes = [E]
     for name in ("astrosim_ensemble_create", "astrosim_ensemble_step", "astrosim_ensemble_summary",
                  "astrosim_ensemble_get_state", "astrosim_ensemble_spike_counts", "astrosim_ensemble_last_step_ms",
-                 "astrosim_ensemble_build_seconds", "astrosim_ensemble_destroy"):
+                 "astrosim_ensemble_build_seconds", "astrosim_ensemble_shared_constants",
+                 "astrosim_ensemble_destroy"):
         getattr(L, name).restype = C.c_int
     S = C.c_void_p
     L.astrosim_server_create.argtypes = [C.c_int, C.c_int, C.c_uint64, C.c_int, C.POINTER(S)]
@@ -331,6 +333,12 @@ class Ensemble:
         s = C.c_double()
         check(lib().astrosim_ensemble_build_seconds(self._h, C.byref(s)))
         return s.value
+
+    def shared_constants(self):
+        """True when the networks differ only in seed, sizes, drive rates and w_a2n."""
+        v = C.c_int()
+        check(lib().astrosim_ensemble_shared_constants(self._h, C.byref(v)))
+        return bool(v.value)
 
 
 class Server:

@@ -250,6 +250,13 @@ int astrosim_ensemble_build_seconds(astrosim_ensemble* e, double* seconds) {
     return ASTROSIM_OK;
 }
 
+int astrosim_ensemble_shared_constants(astrosim_ensemble* e, int* shared) {
+    if (!e || !shared) return fail(ASTROSIM_ERR_INVALID_ARG, "null argument");
+    *shared = e->ens.uniform_constants() ? 1 : 0;
+    g_last_error.clear();
+    return ASTROSIM_OK;
+}
+
 int astrosim_ensemble_destroy(astrosim_ensemble* e) {
     delete e;
     g_last_error.clear();

@@ -15,7 +15,7 @@ namespace {
 
 template <typename R>
 struct alignas(16) NetDesc {
-    RunConsts rc;
+    NetScalars ns;  // the constants that differ between networks
     StepPtrs<R> p;
     WinPtrs<R> w;
     i64 mark;  // last step of the pre-run (src/astrosim_fused.cu:1066)
@@ -27,13 +27,20 @@ constexpr int kEnsTuneRounds = 2;
 constexpr int kGraphWindows = 10;
 constexpr u32 kPushBlocksPerNet = 4;
 
-template <typename R, int MB>
-__global__ void __launch_bounds__(128, MB) ens_window_kernel(const NetDesc<R>* __restrict__ descs,
+// One window of one 128-cell tile.  UNI: every network shares the constants outside
+// NetScalars, which then come from the kernel parameters (`common`); otherwise each
+// block also stages its network's full constants (`rcs`) into shared memory.
+template <typename R, int MB, bool UNI>
+__global__ void __launch_bounds__(128, MB) ens_window_kernel(RunConsts common, const RunConsts* __restrict__ rcs,
+                                                             const NetDesc<R>* __restrict__ descs,
                                                              const u32* __restrict__ tile_net,
                                                              const u32* __restrict__ tile_blk,
                                                              const i64* __restrict__ win,
                                                              const i64* __restrict__ stop, int W) {
-    __shared__ __align__(16) unsigned char smem[sizeof(NetDesc<R>)];
+    constexpr u32 kDescBytes = sizeof(NetDesc<R>);
+    constexpr u32 kConstBytes = UNI ? 0 : sizeof(RunConsts);
+    static_assert(kDescBytes % 16 == 0 && sizeof(RunConsts) % 16 == 0, "16-byte staging");
+    __shared__ __align__(16) unsigned char smem[kDescBytes + kConstBytes];
     const u32 net = tile_net[blockIdx.x];
     const i64 k = win[net];
     const i64 start = k * W;
@@ -42,14 +49,25 @@ __global__ void __launch_bounds__(128, MB) ens_window_kernel(const NetDesc<R>* _
     {
         const uint4* src = reinterpret_cast<const uint4*>(descs + net);
         uint4* dst = reinterpret_cast<uint4*>(smem);
-        for (u32 i = threadIdx.x; i < sizeof(NetDesc<R>) / sizeof(uint4); i += blockDim.x) dst[i] = src[i];
+        for (u32 i = threadIdx.x; i < kDescBytes / 16; i += blockDim.x) dst[i] = src[i];
+        if constexpr (!UNI) {
+            const uint4* rsrc = reinterpret_cast<const uint4*>(rcs + net);
+            uint4* rdst = reinterpret_cast<uint4*>(smem + kDescBytes);
+            for (u32 i = threadIdx.x; i < kConstBytes / 16; i += blockDim.x) rdst[i] = rsrc[i];
+        }
     }
     __syncthreads();
     const NetDesc<R>& d = *reinterpret_cast<const NetDesc<R>*>(smem);
     const int s_end = static_cast<int>(end - start < W ? end - start : W);
     const u32 tb = tile_blk[blockIdx.x];
-    window_cells<R>(d.rc, d.p, d.w, start, 0, s_end, static_cast<int>(k & 1), d.mark, tb & 0x7FFFFFFFu,
-                    (tb >> 31) != 0);
+    if constexpr (UNI) {
+        window_cells<R>(common, d.ns, d.p, d.w, start, 0, s_end, static_cast<int>(k & 1), d.mark, tb & 0x7FFFFFFFu,
+                        (tb >> 31) != 0);
+    } else {
+        const RunConsts& rc = *reinterpret_cast<const RunConsts*>(smem + kDescBytes);
+        window_cells<R>(rc, d.ns, d.p, d.w, start, 0, s_end, static_cast<int>(k & 1), d.mark, tb & 0x7FFFFFFFu,
+                        (tb >> 31) != 0);
+    }
 }
 
 template <typename R>
@@ -59,7 +77,7 @@ __global__ void ens_push_kernel(const NetDesc<R>* __restrict__ descs, const i64*
     const i64 k = win[net];
     if (k * W + W > stop[net]) return;  // the window did not complete: no window follows it
     const NetDesc<R>& d = descs[net];
-    push_cells<R>(d.w, d.rc.n_exc, d.rc.n_neurons - d.rc.n_exc, d.rc.n_neurons, d.rc.n_astro,
+    push_cells<R>(d.w, d.ns.n_exc, d.ns.n_neurons - d.ns.n_exc, d.ns.n_neurons, d.ns.n_astro,
                   static_cast<int>(k & 1), blockIdx.x, gridDim.x);
 }
 
@@ -68,32 +86,76 @@ __global__ void ens_advance_kernel(i64* win, const i64* stop, u32 n, int W) {
     if (i < n && win[i] * W < stop[i]) win[i] += 1;
 }
 
-template <typename R>
-void launch_ens_window(int v, u32 grid, cudaStream_t st, const NetDesc<R>* d, const u32* tn, const u32* tb,
-                       const i64* win, const i64* stop, int W) {
+template <typename R, bool UNI>
+void launch_ens_window_v(int v, u32 grid, cudaStream_t st, const RunConsts& common, const RunConsts* rcs,
+                         const NetDesc<R>* d, const u32* tn, const u32* tb, const i64* win, const i64* stop, int W) {
     switch (kEnsVariants[v]) {
-        case 4: ens_window_kernel<R, 4><<<grid, 128, 0, st>>>(d, tn, tb, win, stop, W); break;
-        case 8: ens_window_kernel<R, 8><<<grid, 128, 0, st>>>(d, tn, tb, win, stop, W); break;
-        default: ens_window_kernel<R, 6><<<grid, 128, 0, st>>>(d, tn, tb, win, stop, W); break;
+        case 4: ens_window_kernel<R, 4, UNI><<<grid, 128, 0, st>>>(common, rcs, d, tn, tb, win, stop, W); break;
+        case 8: ens_window_kernel<R, 8, UNI><<<grid, 128, 0, st>>>(common, rcs, d, tn, tb, win, stop, W); break;
+        default: ens_window_kernel<R, 6, UNI><<<grid, 128, 0, st>>>(common, rcs, d, tn, tb, win, stop, W); break;
     }
 }
 
+// One window and its push for every network.
 template <typename R>
-Status build_descs(std::vector<std::unique_ptr<Simulation>>& nets, DevBuf<unsigned char>& descs, cudaStream_t st) {
+void launch_ens_window(int v, bool uniform, u32 grid, u32 n, cudaStream_t st, const RunConsts& common,
+                       const void* rcs, const void* descs, const u32* tn, const u32* tb, const i64* win,
+                       const i64* stop, int W) {
+    const RunConsts* r = static_cast<const RunConsts*>(rcs);
+    const NetDesc<R>* d = static_cast<const NetDesc<R>*>(descs);
+    if (uniform) launch_ens_window_v<R, true>(v, grid, st, common, r, d, tn, tb, win, stop, W);
+    else launch_ens_window_v<R, false>(v, grid, st, common, r, d, tn, tb, win, stop, W);
+    ens_push_kernel<R><<<dim3(kPushBlocksPerNet, n), 256, 0, st>>>(d, win, stop, W);
+}
+
+// `rc` with the NetScalars fields cleared.  RunConsts has no implicit padding, so
+// equal constants compare equal bytewise; a signed zero that differs only sends a
+// batch to the staged-constants kernel, never the reverse.
+RunConsts common_part(const RunConsts& rc) {
+    RunConsts m;
+    std::memcpy(static_cast<void*>(&m), &rc, sizeof(RunConsts));
+    m.seed = 0;
+    m.n_exc = m.n_neurons = m.n_astro = m.words = 0;
+    m.lambda_astro = m.limit_astro = m.lambda_exc = m.limit_exc = m.lambda_inh = m.limit_inh = 0.0;
+    m.lim53_astro = m.lim53_exc = m.lim53_inh = 0;
+    m.w_a2n = 0.0;
+    m.f_w_a2n = 0.0f;
+    return m;
+}
+
+template <typename R>
+Status build_descs(std::vector<std::unique_ptr<Simulation>>& nets, DevBuf<unsigned char>& descs,
+                   DevBuf<unsigned char>& rcs, RunConsts& common, bool& uniform, cudaStream_t st) {
     std::vector<NetDesc<R>> h(nets.size());
+    std::vector<RunConsts> hr(nets.size());
     std::memset(static_cast<void*>(h.data()), 0, h.size() * sizeof(NetDesc<R>));
+    std::memset(static_cast<void*>(hr.data()), 0, hr.size() * sizeof(RunConsts));
+    bool first = true;
+    uniform = true;
+    std::memset(static_cast<void*>(&common), 0, sizeof(RunConsts));
     for (size_t i = 0; i < nets.size(); ++i) {
         Simulation* s = nets[i].get();
         if (!s) continue;
         const RunConsts& rc = s->consts();
-        h[i].rc = rc;
+        std::memcpy(static_cast<void*>(&hr[i]), &rc, sizeof(RunConsts));
+        const RunConsts c = common_part(rc);
+        if (first) {
+            std::memcpy(static_cast<void*>(&common), &c, sizeof(RunConsts));
+            first = false;
+        } else if (std::memcmp(&common, &c, sizeof(RunConsts)) != 0) {
+            uniform = false;
+        }
+        h[i].ns = net_scalars(rc);
         h[i].p = make_ptrs<R>(s->state_buffers(), s->network(), rc, s->raster_steps());
         h[i].w = win_ptrs<R>(*s->window_state(), rc);
         h[i].mark = s->pre_steps() == 0 ? 0 : s->pre_steps() - 1;
     }
     AS_TRY(descs.alloc(std::max<size_t>(1, h.size()) * sizeof(NetDesc<R>)));
-    if (!h.empty())
+    AS_TRY(rcs.alloc(std::max<size_t>(1, hr.size()) * sizeof(RunConsts)));
+    if (!h.empty()) {
         AS_CUDA(cudaMemcpyAsync(descs.get(), h.data(), h.size() * sizeof(NetDesc<R>), cudaMemcpyHostToDevice, st));
+        AS_CUDA(cudaMemcpyAsync(rcs.get(), hr.data(), hr.size() * sizeof(RunConsts), cudaMemcpyHostToDevice, st));
+    }
     AS_CUDA(cudaStreamSynchronize(st));
     return Status::Ok();
 }
@@ -107,6 +169,7 @@ Ensemble::~Ensemble() {
     if (ev1_) cudaEventDestroy(ev1_);
     nets_.clear();
     descs_.release();
+    rcs_.release();
     tile_net_.release();
     tile_blk_.release();
     win_.release();
@@ -180,8 +243,8 @@ Status Ensemble::create(const astrosim_config* cfgs, u32 n, const char* const* b
 Status Ensemble::rebuild() {
     AS_CUDA(cudaSetDevice(device_));
     AllocStream alloc_scope(stream_);
-    if (fp32_) AS_TRY(build_descs<float>(nets_, descs_, stream_));
-    else AS_TRY(build_descs<double>(nets_, descs_, stream_));
+    if (fp32_) AS_TRY(build_descs<float>(nets_, descs_, rcs_, common_, uniform_, stream_));
+    else AS_TRY(build_descs<double>(nets_, descs_, rcs_, common_, uniform_, stream_));
     std::vector<u32> tn, tb;
     for (u32 i = 0; i < nets_.size(); ++i) {
         if (!nets_[i]) continue;
@@ -211,24 +274,23 @@ Status Ensemble::rebuild() {
     return Status::Ok();
 }
 
+void Ensemble::launch_window(int v) {
+    const u32 n = static_cast<u32>(nets_.size());
+    if (fp32_)
+        launch_ens_window<float>(v, uniform_, n_tiles_, n, stream_, common_, rcs_.get(), descs_.get(), tile_net_.get(),
+                                 tile_blk_.get(), win_.get(), stop_.get(), W_);
+    else
+        launch_ens_window<double>(v, uniform_, n_tiles_, n, stream_, common_, rcs_.get(), descs_.get(),
+                                  tile_net_.get(), tile_blk_.get(), win_.get(), stop_.get(), W_);
+}
+
 Status Ensemble::capture_graph() {
     if (graph_) return Status::Ok();
     const u32 n = static_cast<u32>(nets_.size());
     cudaGraph_t g = nullptr;
     AS_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < kGraphWindows; ++k) {
-        if (fp32_) {
-            launch_ens_window<float>(variant_, n_tiles_, stream_, reinterpret_cast<const NetDesc<float>*>(descs_.get()),
-                                     tile_net_.get(), tile_blk_.get(), win_.get(), stop_.get(), W_);
-            ens_push_kernel<float><<<dim3(kPushBlocksPerNet, n), 256, 0, stream_>>>(
-                reinterpret_cast<const NetDesc<float>*>(descs_.get()), win_.get(), stop_.get(), W_);
-        } else {
-            launch_ens_window<double>(variant_, n_tiles_, stream_,
-                                      reinterpret_cast<const NetDesc<double>*>(descs_.get()), tile_net_.get(),
-                                      tile_blk_.get(), win_.get(), stop_.get(), W_);
-            ens_push_kernel<double><<<dim3(kPushBlocksPerNet, n), 256, 0, stream_>>>(
-                reinterpret_cast<const NetDesc<double>*>(descs_.get()), win_.get(), stop_.get(), W_);
-        }
+        launch_window(variant_);
         ens_advance_kernel<<<ceil_div(n, 256), 256, 0, stream_>>>(win_.get(), stop_.get(), n, W_);
     }
     const cudaError_t e = cudaStreamEndCapture(stream_, &g);
@@ -255,17 +317,7 @@ Status Ensemble::advance_windows(i64 windows) {
     AS_CUDA(cudaEventRecord(ev0_, stream_));
     i64 done = 0;
     auto one_window = [&](int v) -> Status {
-        if (fp32_) {
-            launch_ens_window<float>(v, n_tiles_, stream_, reinterpret_cast<const NetDesc<float>*>(descs_.get()),
-                                     tile_net_.get(), tile_blk_.get(), win_.get(), stop_.get(), W_);
-            ens_push_kernel<float><<<dim3(kPushBlocksPerNet, n), 256, 0, stream_>>>(
-                reinterpret_cast<const NetDesc<float>*>(descs_.get()), win_.get(), stop_.get(), W_);
-        } else {
-            launch_ens_window<double>(v, n_tiles_, stream_, reinterpret_cast<const NetDesc<double>*>(descs_.get()),
-                                      tile_net_.get(), tile_blk_.get(), win_.get(), stop_.get(), W_);
-            ens_push_kernel<double><<<dim3(kPushBlocksPerNet, n), 256, 0, stream_>>>(
-                reinterpret_cast<const NetDesc<double>*>(descs_.get()), win_.get(), stop_.get(), W_);
-        }
+        launch_window(v);
         ens_advance_kernel<<<ceil_div(n, 256), 256, 0, stream_>>>(win_.get(), stop_.get(), n, W_);
         AS_CUDA(cudaGetLastError());
         return Status::Ok();

@@ -4,7 +4,10 @@
 // windowed engine buffers).  One window launch covers every cell of every network:
 // a tile table maps each 128-cell block to (network, population, block), and each
 // block reads its network's descriptor (constants and pointers) into shared memory.
-// Every network has its own window counter and stop step on the device, so the
+// The constants that differ between networks (NetScalars) sit in the descriptor;
+// when every network shares the rest (the same biology, dt and substeps) those come
+// from the kernel parameters, else each block also stages its network's full
+// constants.  Every network has its own window counter and stop step on the device, so the
 // per-window sequence {window, push, advance} is identical for every window and is
 // captured once in a CUDA graph and replayed.
 #pragma once
@@ -27,6 +30,7 @@ public:
     Status spike_counts(u32 i, i64 first, i64 n, u32* dst);
     Status last_step_ms(double* ms);
     u32 size() const { return static_cast<u32>(nets_.size()); }
+    bool uniform_constants() const { return uniform_; }
     i64 steps_done() const { return steps_done_; }
     double build_seconds() const { return build_seconds_; }
 
@@ -44,6 +48,7 @@ private:
     Status rebuild();
     Status capture_graph();
     Status sync_progress();
+    void launch_window(int v);  // window + push kernels for variant v
 
     std::vector<std::unique_ptr<Simulation>> nets_;
     std::vector<i64> win_host_;  // window index of each network at the last sync
@@ -54,6 +59,9 @@ private:
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     bool have_events_ = false;
     DevBuf<unsigned char> descs_;
+    DevBuf<unsigned char> rcs_;  // RunConsts per network (read when !uniform_)
+    RunConsts common_{};         // shared constants (NetScalars fields cleared)
+    bool uniform_ = true;
     DevBuf<u32> tile_net_, tile_blk_;
     DevBuf<i64> win_, stop_;
     u32 n_tiles_ = 0;

@@ -165,8 +165,10 @@ struct AstroK {
     float f_inv_ratio, f_ratio_rate_IP3R, f_ratio_rate_L, f_k_Kd_inh, f_Km2;
     // Float copies read by the FP32 stages (converted once here, not per use).
     float f_Kd_IP3_1, f_Kd_IP3_2, f_Kd_act, f_rate_SERCA, f_k_IP3R, f_SIC_scale;
+    float pad_;        // explicit, zero: the struct has no implicit padding
     double rcp_ratio;  // RN(1 / ratio_ER_cyt), for the exact division by a constant (div_by)
 };
+static_assert(sizeof(AstroK) == 12 * 8 + 12 * 4 + 8, "AstroK has no implicit padding");
 
 // AdEx neuron constants for one population (src/astrosim_fused.cu:228-232).
 struct NeuronK {
@@ -183,9 +185,11 @@ struct NeuronK {
     // Refractory length in steps, static_cast<int>(t_ref / h_step + 0.5) (src/astrosim_fused.cu:555);
     // set with the step size.
     int ref_steps;
+    int pad_;  // explicit, zero: the struct has no implicit padding
     // RN(1 / x) of the constant divisors, for the exact division by a constant (div_by).
     double rcp_C_m, rcp_tau_w, rcp_Delta_T;
 };
+static_assert(sizeof(NeuronK) == 17 * 8 + 14 * 4 + 2 * 4 + 3 * 8, "NeuronK has no implicit padding");
 
 // Biology defaults, compiled into the reference (src/astrosim_fused.cu:742-781).
 struct Biology {

@@ -31,7 +31,7 @@ __global__ void __launch_bounds__(128, MB) shard_window_kernel(RunConsts rc, Ste
                                                                i64 win_start, int buf, i64 mark, u32 a_blk0,
                                                                u32 a_nblk, u32 n_blk0) {
     const bool astro = blockIdx.x < a_nblk;
-    window_cells<R>(rc, p, w, win_start, 0, w.W, buf, mark, astro ? a_blk0 + blockIdx.x : n_blk0 + (blockIdx.x - a_nblk),
+    window_cells<R>(rc, net_scalars(rc), p, w, win_start, 0, w.W, buf, mark, astro ? a_blk0 + blockIdx.x : n_blk0 + (blockIdx.x - a_nblk),
                     astro);
 }
 

@@ -29,15 +29,16 @@ namespace {
 template <typename R>
 __global__ void fused_step_kernel(RunConsts rc, StepPtrs<R> p, i64 step, u32 astro_blocks,
                                                          int sic_refresh, u64 noise_idx) {
+    const NetScalars ns = net_scalars(rc);
     if (blockIdx.x < astro_blocks) {
         const u32 a = blockIdx.x * blockDim.x + threadIdx.x;
-        if (a < rc.n_astro) astro_cell_step<R>(rc, p, a, step);
+        if (a < rc.n_astro) astro_cell_step<R>(rc, ns, p, a, step);
         return;
     }
     const u32 j = (blockIdx.x - astro_blocks) * blockDim.x + threadIdx.x;
     R out = static_cast<R>(0.0);
     bool spiked = false;
-    if (j < rc.n_neurons) spiked = neuron_cell_step<R>(rc, p, j, step, sic_refresh != 0, noise_idx, out);
+    if (j < rc.n_neurons) spiked = neuron_cell_step<R>(rc, ns, p, j, step, sic_refresh != 0, noise_idx, out);
     // pack this warp's 32 spike bits into one word of the ring (warps cover aligned 32-neuron groups)
     const unsigned ballot = __ballot_sync(0xffffffffu, spiked);
     const int S = rc.slots;

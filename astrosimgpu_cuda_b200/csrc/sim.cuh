@@ -20,6 +20,7 @@ struct RunConsts {
     int d_e, d_i, d_a2n, slots;
     int steps_per_noise;
     int sic_interval;
+    int pad0_;  // explicit padding, zero (see the size check below)
     double w_e, w_i, w_n2a, w_a2n;
     double lambda_astro, limit_astro, weight_astro, noise_astro;
     double lambda_exc, limit_exc, weight_exc, noise_exc;
@@ -27,6 +28,7 @@ struct RunConsts {
     u64 lim53_astro, lim53_exc, lim53_inh;  // floor(exp(-lambda) * 2^53) for the integer first test
     bool independent_noise;
     bool stp_enabled;
+    bool pad1_[6];
     double stp_U, stp_tau_rec, stp_tau_fac;
     double SIC_th;
     u64 seed;
@@ -37,6 +39,46 @@ struct RunConsts {
     float f_h_step, f_h6, f_w_e, f_neg_w_i, f_w_n2a, f_w_a2n;
     float f_weight_astro, f_weight_exc, f_weight_inh, f_noise_astro;
 };
+// Every byte of RunConsts is a member (the padding is explicit and zero), so two
+// copies built from the same values compare equal bytewise; the batched engine
+// relies on that to find networks that share their constants.
+static_assert(sizeof(RunConsts) == sizeof(AstroK) + 2 * sizeof(NeuronK) + 2 * 8 + 8 * 4 + 16 * 8 + 3 * 8 + 8 +
+                                       5 * 8 + 4 * 4 + 8 + 10 * 4,
+              "RunConsts has no implicit padding");
+
+// The run constants that differ between the networks of a batch (seed, sizes,
+// drive rates, astrocyte-to-neuron weight).  Everything else in RunConsts is the
+// same for networks built with the same biology, so a batched launch can read it
+// from its kernel parameters and only these from each network's descriptor.
+struct NetScalars {
+    u64 seed;
+    u32 n_exc, n_neurons, n_astro, words;
+    double lambda_astro, limit_astro, lambda_exc, limit_exc, lambda_inh, limit_inh;
+    u64 lim53_astro, lim53_exc, lim53_inh;
+    double w_a2n;
+    float f_w_a2n;
+};
+
+__host__ __device__ __forceinline__ NetScalars net_scalars(const RunConsts& rc) {
+    NetScalars n{};
+    n.seed = rc.seed;
+    n.n_exc = rc.n_exc;
+    n.n_neurons = rc.n_neurons;
+    n.n_astro = rc.n_astro;
+    n.words = rc.words;
+    n.lambda_astro = rc.lambda_astro;
+    n.limit_astro = rc.limit_astro;
+    n.lambda_exc = rc.lambda_exc;
+    n.limit_exc = rc.limit_exc;
+    n.lambda_inh = rc.lambda_inh;
+    n.limit_inh = rc.limit_inh;
+    n.lim53_astro = rc.lim53_astro;
+    n.lim53_exc = rc.lim53_exc;
+    n.lim53_inh = rc.lim53_inh;
+    n.w_a2n = rc.w_a2n;
+    n.f_w_a2n = rc.f_w_a2n;
+    return n;
+}
 
 // Derives the stage-type copies in `rc` from its double fields.  Every value equals
 // what the device would compute from the double (host and device division and

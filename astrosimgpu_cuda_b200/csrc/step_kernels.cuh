@@ -128,18 +128,18 @@ __device__ __forceinline__ void astro_advance(const AstroK& c, AstroRegs<R>& s, 
 // Everything astrocyte `a` does in step `step` once its delayed spike sum is known
 // (src/astrosim_fused.cu:390-417): Poisson IP3 drive, noise, RK4, SIC factor.
 template <typename R>
-__device__ __forceinline__ R astro_advance_step(const RunConsts& rc, AstroRegs<R>& s, R gathered, u32 a, i64 step,
+__device__ __forceinline__ R astro_advance_step(const RunConsts& rc, const NetScalars& ns, AstroRegs<R>& s, R gathered, u32 a, i64 step,
                                                 u64 poisson_base, u64 noise_base) {
     R ip3_input = as_r<R>(rc.w_n2a, rc.f_w_n2a) * gathered;
-    if (rc.lambda_astro > 0.0) {
-        const int ev = rng_poisson_at(poisson_base, rc.lambda_astro, rc.limit_astro, rc.lim53_astro);
+    if (ns.lambda_astro > 0.0) {
+        const int ev = rng_poisson_at(poisson_base, ns.lambda_astro, ns.limit_astro, ns.lim53_astro);
         if (ev > 0) ip3_input += as_r<R>(rc.weight_astro, rc.f_weight_astro) * static_cast<R>(ev);
     }
     R noise = static_cast<R>(0.0);
     if (rc.noise_astro > 0.0) {
         u64 base = noise_base;
         if (!rc.independent_noise)
-            base = rng_base(rc.seed ^ kAstroNoiseKey, static_cast<u64>(step / rc.steps_per_noise));
+            base = rng_base(ns.seed ^ kAstroNoiseKey, static_cast<u64>(step / rc.steps_per_noise));
         if constexpr (std::is_same<R, float>::value) {
             noise = rc.f_noise_astro * normal_fast(base);
         } else {
@@ -167,20 +167,21 @@ __device__ __forceinline__ u64 step_base(u64 seed, u64 key, i64 step, u32 cell) 
 
 // One astrocyte for step `step` on the per-step rings (src/astrosim_fused.cu:374-427).
 template <typename R>
-__device__ __forceinline__ void astro_cell_step(const RunConsts& rc, const StepPtrs<R>& p, u32 a, i64 step) {
+__device__ __forceinline__ void astro_cell_step(const RunConsts& rc, const NetScalars& ns, const StepPtrs<R>& p, u32 a,
+                                                i64 step) {
     const int S = rc.slots;
     const int read_slot = static_cast<int>((step + S - rc.d_e) % S);  // the e2a delay is d_e (384)
-    const R gathered = gather_spikes<R>(p.e2a_rs, p.e2a_src, a, p.bits + static_cast<u64>(read_slot) * rc.words,
-                                        p.val + static_cast<u64>(read_slot) * rc.n_neurons);
+    const R gathered = gather_spikes<R>(p.e2a_rs, p.e2a_src, a, p.bits + static_cast<u64>(read_slot) * ns.words,
+                                        p.val + static_cast<u64>(read_slot) * ns.n_neurons);
     AstroRegs<R> s = load_astro<R>(p.Ca[a], p.IP3[a], p.h[a], p.Ca_tot[a], p.IP3_0[a], p.tau_IP3[a], p.delta_IP3[a]);
-    const R factor = astro_advance_step<R>(rc, s, gathered, a, step, step_base(rc.seed, kAstroPoissonKey, step, a),
-                                           step_base(rc.seed, kAstroNoiseKey, step, a));
+    const R factor = astro_advance_step<R>(rc, ns, s, gathered, a, step, step_base(ns.seed, kAstroPoissonKey, step, a),
+                                           step_base(ns.seed, kAstroNoiseKey, step, a));
     p.Ca[a] = s.Ca;
     p.IP3[a] = s.IP3;
     p.h[a] = s.h;
     if (p.ca_rec) record_ca<R>(p, a, step, (step + 1) % p.rec_every == 0, s.Ca);
     if (factor > static_cast<R>(0.0)) p.ever_active[a] = 1;
-    p.sic_ring[static_cast<u64>(step % S) * rc.n_astro + a] = factor;
+    p.sic_ring[static_cast<u64>(step % S) * ns.n_astro + a] = factor;
     p.sic_last[a] = factor;
 }
 
@@ -197,21 +198,22 @@ struct NeuronRegs {
 // noise, the alpha-cascade closed form and AdEx RK4 (or the refractory Euler step),
 // the spike test.  `noise` is noise_std * N(0,1) for this step when `has_noise`.
 template <typename R>
-__device__ __forceinline__ bool neuron_advance_step(const RunConsts& rc, const NeuronK& pk, bool excitatory,
+__device__ __forceinline__ bool neuron_advance_step(const RunConsts& rc, const NetScalars& ns, const NeuronK& pk,
+                                                    bool excitatory,
                                                     NeuronRegs<R>& n, R exc_sum, R inh_sum, bool sic_refresh,
                                                     R sic_sum, bool has_noise, double noise, u64 poisson_base,
                                                     R ex_decay, R in_decay) {
     R exc_input = as_r<R>(rc.w_e, rc.f_w_e) * exc_sum;
     const R inh_input = as_r<R>(-rc.w_i, rc.f_neg_w_i) * inh_sum;
-    const double lambda = excitatory ? rc.lambda_exc : rc.lambda_inh;
+    const double lambda = excitatory ? ns.lambda_exc : ns.lambda_inh;
     if (lambda > 0.0) {
-        const int ev = rng_poisson_at(poisson_base, lambda, excitatory ? rc.limit_exc : rc.limit_inh,
-                                      excitatory ? rc.lim53_exc : rc.lim53_inh);
+        const int ev = rng_poisson_at(poisson_base, lambda, excitatory ? ns.limit_exc : ns.limit_inh,
+                                      excitatory ? ns.lim53_exc : ns.lim53_inh);
         if (ev > 0)
             exc_input += (excitatory ? as_r<R>(rc.weight_exc, rc.f_weight_exc) : as_r<R>(rc.weight_inh, rc.f_weight_inh)) *
                          static_cast<R>(ev);
     }
-    if (sic_refresh) n.I_sic = as_r<R>(rc.w_a2n, rc.f_w_a2n) * sic_sum;
+    if (sic_refresh) n.I_sic = as_r<R>(ns.w_a2n, ns.f_w_a2n) * sic_sum;
     R I_ext = n.I_sic;
     if (has_noise) I_ext += static_cast<R>(noise);
 
@@ -289,8 +291,8 @@ __device__ __forceinline__ R stp_on_spike(const RunConsts& rc, R& sx, R& su, dou
 
 // noise_std * N(0,1) of neuron j for noise index idx (src/astrosim_fused.cu:494-504).
 template <typename R>
-__device__ __forceinline__ double neuron_noise(const RunConsts& rc, double nstd, u64 idx, u32 j) {
-    const u64 base = rng_base(rc.seed ^ kNeuronNoiseKey, idx * kNoiseStride + j);
+__device__ __forceinline__ double neuron_noise(const NetScalars& ns, double nstd, u64 idx, u32 j) {
+    const u64 base = rng_base(ns.seed ^ kNeuronNoiseKey, idx * kNoiseStride + j);
     if constexpr (std::is_same<R, float>::value) {
         return static_cast<double>(static_cast<float>(nstd) * normal_fast(base));
     } else {
@@ -304,35 +306,36 @@ __device__ __forceinline__ double neuron_noise(const RunConsts& rc, double nstd,
 // One neuron for step `step` on the per-step rings (src/astrosim_fused.cu:433-587).
 // Returns whether it spiked and the value its ring entry carries.
 template <typename R>
-__device__ __forceinline__ bool neuron_cell_step(const RunConsts& rc, const StepPtrs<R>& p, u32 j, i64 step,
+__device__ __forceinline__ bool neuron_cell_step(const RunConsts& rc, const NetScalars& ns, const StepPtrs<R>& p, u32 j,
+                                                 i64 step,
                                                  bool sic_refresh, u64 noise_idx, R& out_value) {
     const int S = rc.slots;
-    const bool excitatory = j < rc.n_exc;
+    const bool excitatory = j < ns.n_exc;
     const NeuronK& pk = excitatory ? rc.pe : rc.pi;
     const int slot_ex = static_cast<int>((step + S - rc.d_e) % S);
     const int slot_in = static_cast<int>((step + S - rc.d_i) % S);
-    const R exc_sum = gather_spikes<R>(p.exc_rs, p.exc_src, j, p.bits + static_cast<u64>(slot_ex) * rc.words,
-                                       p.val + static_cast<u64>(slot_ex) * rc.n_neurons);
+    const R exc_sum = gather_spikes<R>(p.exc_rs, p.exc_src, j, p.bits + static_cast<u64>(slot_ex) * ns.words,
+                                       p.val + static_cast<u64>(slot_ex) * ns.n_neurons);
     // inh sources are local inhibitory indices that index the ring by global id (458-463)
-    const R inh_sum = gather_spikes<R>(p.inh_rs, p.inh_src, j, p.bits + static_cast<u64>(slot_in) * rc.words,
-                                       p.val + static_cast<u64>(slot_in) * rc.n_neurons);
+    const R inh_sum = gather_spikes<R>(p.inh_rs, p.inh_src, j, p.bits + static_cast<u64>(slot_in) * ns.words,
+                                       p.val + static_cast<u64>(slot_in) * ns.n_neurons);
     R sic_sum = static_cast<R>(0.0);
     if (sic_refresh) {
         const int slot_sic = static_cast<int>((step + S - rc.d_a2n) % S);
-        const R* row = p.sic_ring + static_cast<u64>(slot_sic) * rc.n_astro;
+        const R* row = p.sic_ring + static_cast<u64>(slot_sic) * ns.n_astro;
         const u32 k1 = p.sic_rs[j + 1];
         for (u32 k = p.sic_rs[j]; k < k1; ++k) sic_sum += row[p.sic_src[k]];
     }
     const double nstd = excitatory ? rc.noise_exc : rc.noise_inh;
     const bool has_noise = nstd > 0.0 && rc.independent_noise;
-    const double noise = has_noise ? neuron_noise<R>(rc, nstd, noise_idx, j) : 0.0;
+    const double noise = has_noise ? neuron_noise<R>(ns, nstd, noise_idx, j) : 0.0;
     NeuronRegs<R> n{p.V[j], p.w[j], p.V_reset[j], p.b[j], p.g_ex[j], p.dg_ex[j], p.g_in[j], p.dg_in[j], p.I_sic[j],
                     p.refr[j]};
     const R hs = as_r<R>(rc.h_step, rc.f_h_step);
     const R ex_decay = exp_r(-hs / static_cast<R>(pk.tau_syn_ex));
     const R in_decay = exp_r(-hs / static_cast<R>(pk.tau_syn_in));
-    const bool spiked = neuron_advance_step<R>(rc, pk, excitatory, n, exc_sum, inh_sum, sic_refresh, sic_sum,
-                                               has_noise, noise, step_base(rc.seed, kNeuronPoissonKey, step, j),
+    const bool spiked = neuron_advance_step<R>(rc, ns, pk, excitatory, n, exc_sum, inh_sum, sic_refresh, sic_sum,
+                                               has_noise, noise, step_base(ns.seed, kNeuronPoissonKey, step, j),
                                                ex_decay, in_decay);
     p.V[j] = n.V;
     p.w[j] = n.w;

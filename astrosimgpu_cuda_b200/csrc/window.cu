@@ -25,7 +25,7 @@ __global__ void __launch_bounds__(128, MinBlocks) window_kernel(RunConsts rc, St
                                                                 i64 win_start, int s_begin, int s_end, int buf,
                                                                 i64 mark, u32 astro_blocks) {
     const bool astro = blockIdx.x < astro_blocks;
-    window_cells<R>(rc, p, w, win_start, s_begin, s_end, buf, mark, astro ? blockIdx.x : blockIdx.x - astro_blocks,
+    window_cells<R>(rc, net_scalars(rc), p, w, win_start, s_begin, s_end, buf, mark, astro ? blockIdx.x : blockIdx.x - astro_blocks,
                     astro);
 }
 

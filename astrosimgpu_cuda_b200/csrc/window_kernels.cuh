@@ -89,12 +89,13 @@ __device__ __forceinline__ void pull_row(const u32* __restrict__ rs, const u32* 
 
 // Neuron j through steps [s_begin, s_end) of the window starting at win_start.
 template <typename R, bool EXC>
-__device__ __forceinline__ void neuron_window(const RunConsts& rc, const NeuronK& pk, const StepPtrs<R>& p,
+__device__ __forceinline__ void neuron_window(const RunConsts& rc, const NetScalars& ns, const NeuronK& pk,
+                                              const StepPtrs<R>& p,
                                               const WinPtrs<R>& w, u32 j, i64 win_start, int s_begin, int s_end,
                                               int buf, bool pull, bool window_done) {
     const int prev = buf ^ 1;
     const int W = w.W;
-    const u64 nN = rc.n_neurons;
+    const u64 nN = ns.n_neurons;
 
     // synaptic input of the window: deposits (push) or the row walk (pull); steps
     // whose bit in ex_mask / in_mask is clear have none (+0.0)
@@ -133,7 +134,7 @@ __device__ __forceinline__ void neuron_window(const RunConsts& rc, const NeuronK
     bool sic_input = false;
     {
         const u32* act = w.astro_active + static_cast<u64>(prev) * w.astro_words;
-        const R* fac = w.sic_win + static_cast<u64>(prev) * rc.n_astro * W;
+        const R* fac = w.sic_win + static_cast<u64>(prev) * ns.n_astro * W;
         const u32 k1 = p.sic_rs[j + 1];
         for (u32 k = p.sic_rs[j]; k < k1; ++k) {
             const u32 a = p.sic_src[k];
@@ -164,17 +165,17 @@ __device__ __forceinline__ void neuron_window(const RunConsts& rc, const NeuronK
     u64 nidx = static_cast<u64>(t0 / spn);
     int nphase = static_cast<int>(t0 % spn);
     double noise = 0.0;
-    if (has_noise) noise = neuron_noise<R>(rc, nstd, nidx, j);
-    u64 pbase = step_base(rc.seed, kNeuronPoissonKey, t0, j);
+    if (has_noise) noise = neuron_noise<R>(ns, nstd, nidx, j);
+    u64 pbase = step_base(ns.seed, kNeuronPoissonKey, t0, j);
     u32 word = 0;
     R* vout = w.spk_val + static_cast<u64>(buf) * W * nN;
     for (int st = s_begin; st < s_end; ++st) {
         const i64 t = win_start + st;
         const bool refresh = since >= 0 && phase == 0;
-        if (has_noise && nphase == 0 && st != s_begin) noise = neuron_noise<R>(rc, nstd, nidx, j);
+        if (has_noise && nphase == 0 && st != s_begin) noise = neuron_noise<R>(ns, nstd, nidx, j);
         const R zero = static_cast<R>(0.0);
         const bool spiked = neuron_advance_step<R>(
-            rc, pk, EXC, n, ((ex_mask >> st) & 1u) ? ex_acc[st] : zero, ((in_mask >> st) & 1u) ? in_acc[st] : zero,
+            rc, ns, pk, EXC, n, ((ex_mask >> st) & 1u) ? ex_acc[st] : zero, ((in_mask >> st) & 1u) ? in_acc[st] : zero,
             refresh, sic_input ? sic_acc[st] : zero, has_noise, noise, pbase, ex_decay, in_decay);
         pbase += kStepAdvance;
         ++since;
@@ -190,7 +191,7 @@ __device__ __forceinline__ void neuron_window(const RunConsts& rc, const NeuronK
             const u32 slot = atomicAdd(&w.spk_count[buf], 1u);
             if (slot < w.cap) w.spk_list[static_cast<u64>(buf) * w.cap + slot] = (j << 5) | static_cast<u32>(st);
             atomicAdd(&p.counts[t], 1u);
-            if (t < p.raster_steps) atomicOr(&p.raster[static_cast<u64>(t) * rc.words + (j >> 5)], 1u << (j & 31));
+            if (t < p.raster_steps) atomicOr(&p.raster[static_cast<u64>(t) * ns.words + (j >> 5)], 1u << (j & 31));
         }
     }
     p.V[j] = n.V;
@@ -209,7 +210,8 @@ __device__ __forceinline__ void neuron_window(const RunConsts& rc, const NeuronK
 // starts at step win_start (buffer parity buf): block `blk` of the astrocytes when
 // `astro`, else block `blk` of the neurons.
 template <typename R>
-__device__ __forceinline__ void window_cells(const RunConsts& rc, const StepPtrs<R>& p, const WinPtrs<R>& w,
+__device__ __forceinline__ void window_cells(const RunConsts& rc, const NetScalars& ns, const StepPtrs<R>& p,
+                                             const WinPtrs<R>& w,
                                              i64 win_start, int s_begin, int s_end, int buf, i64 mark, u32 blk,
                                              bool astro) {
     const int prev = buf ^ 1;
@@ -219,7 +221,7 @@ __device__ __forceinline__ void window_cells(const RunConsts& rc, const StepPtrs
     if (astro) {
         // ------------------------------------------------------------ astrocytes
         const u32 a = blk * blockDim.x + threadIdx.x;
-        const bool valid = a < rc.n_astro;
+        const bool valid = a < ns.n_astro;
         bool any_active = false;
         if (valid) {
             AstroRegs<R> s = load_astro<R>(p.Ca[a], p.IP3[a], p.h[a], p.Ca_tot[a], p.IP3_0[a], p.tau_IP3[a],
@@ -227,13 +229,13 @@ __device__ __forceinline__ void window_cells(const RunConsts& rc, const StepPtrs
             // per-step IP3 input; steps whose bit in in_mask is clear have none (+0.0)
             R acc[kMaxWindow];
             u32 in_mask = 0;
-            const u64 slot_base = (static_cast<u64>(buf) * rc.n_astro + a);
+            const u64 slot_base = (static_cast<u64>(buf) * ns.n_astro + a);
             const u32 c = w.ain_cnt[slot_base];
             if (pull || c > kInboxSlots) {
                 for (int i = 0; i < W; ++i) acc[i] = static_cast<R>(0.0);
                 in_mask = (1u << W) - 1u;
-                pull_row<R>(p.e2a_rs, p.e2a_src, a, w.spk_word + static_cast<u64>(prev) * rc.n_neurons,
-                            w.spk_val + static_cast<u64>(prev) * W * rc.n_neurons, rc.n_neurons, s_begin, s_end, acc);
+                pull_row<R>(p.e2a_rs, p.e2a_src, a, w.spk_word + static_cast<u64>(prev) * ns.n_neurons,
+                            w.spk_val + static_cast<u64>(prev) * W * ns.n_neurons, ns.n_neurons, s_begin, s_end, acc);
             } else if (c > 0) {
                 Deposit<R> d[kInboxSlots];
                 for (u32 i = 0; i < c; ++i) d[i] = w.ain_ent[slot_base * kInboxSlots + i];
@@ -248,15 +250,15 @@ __device__ __forceinline__ void window_cells(const RunConsts& rc, const StepPtrs
             }
             if (window_done && c) w.ain_cnt[slot_base] = 0;
             unsigned char ever = p.ever_active[a];
-            R* out = w.sic_win + (static_cast<u64>(buf) * rc.n_astro + a) * W;
+            R* out = w.sic_win + (static_cast<u64>(buf) * ns.n_astro + a) * W;
             R factor = static_cast<R>(0.0);
-            u64 pbase = step_base(rc.seed, kAstroPoissonKey, win_start + s_begin, a);
-            u64 nbase = step_base(rc.seed, kAstroNoiseKey, win_start + s_begin, a);
+            u64 pbase = step_base(ns.seed, kAstroPoissonKey, win_start + s_begin, a);
+            u64 nbase = step_base(ns.seed, kAstroNoiseKey, win_start + s_begin, a);
             // recording phase (t + 1) % rec_every, advanced by a counter
             i64 rphase = p.ca_rec ? (win_start + s_begin + 1) % p.rec_every : 1;
             for (int st = s_begin; st < s_end; ++st) {
                 const i64 t = win_start + st;
-                factor = astro_advance_step<R>(rc, s, ((in_mask >> st) & 1u) ? acc[st] : static_cast<R>(0.0), a, t,
+                factor = astro_advance_step<R>(rc, ns, s, ((in_mask >> st) & 1u) ? acc[st] : static_cast<R>(0.0), a, t,
                                                pbase, nbase);
                 pbase += kStepAdvance;
                 nbase += kStepAdvance;
@@ -278,7 +280,7 @@ __device__ __forceinline__ void window_cells(const RunConsts& rc, const StepPtrs
             p.sic_last[a] = factor;
         }
         const unsigned ballot = __ballot_sync(0xffffffffu, any_active);
-        if ((threadIdx.x & 31) == 0 && a < rc.n_astro) {
+        if ((threadIdx.x & 31) == 0 && a < ns.n_astro) {
             u32* word = w.astro_active + static_cast<u64>(buf) * w.astro_words + (a >> 5);
             if (s_begin == 0) *word = ballot; else if (ballot) atomicOr(word, ballot);
         }
@@ -286,12 +288,12 @@ __device__ __forceinline__ void window_cells(const RunConsts& rc, const StepPtrs
     }
     // ---------------------------------------------------------------- neurons
     const u32 j = blk * blockDim.x + threadIdx.x;
-    if (j >= rc.n_neurons) return;
+    if (j >= ns.n_neurons) return;
     // one instantiation per population, so its constants are compile-time operands
-    if (j < rc.n_exc)
-        neuron_window<R, true>(rc, rc.pe, p, w, j, win_start, s_begin, s_end, buf, pull, window_done);
+    if (j < ns.n_exc)
+        neuron_window<R, true>(rc, ns, rc.pe, p, w, j, win_start, s_begin, s_end, buf, pull, window_done);
     else
-        neuron_window<R, false>(rc, rc.pi, p, w, j, win_start, s_begin, s_end, buf, pull, window_done);
+        neuron_window<R, false>(rc, ns, rc.pi, p, w, j, win_start, s_begin, s_end, buf, pull, window_done);
 }
 
 // After window `buf` completes: deliver its spikes into the inboxes of the next

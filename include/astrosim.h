@@ -293,6 +293,13 @@ int astrosim_ensemble_last_step_ms(astrosim_ensemble* e, double* ms);
 /* Wall time of astrosim_ensemble_create (all builds), seconds. */
 int astrosim_ensemble_build_seconds(astrosim_ensemble* e, double* seconds);
 
+/* *shared = 1 when every network of the batch has the same constants apart from its
+ * seed, sizes, drive rates and astrocyte-to-neuron weight (the window launch then
+ * passes the shared constants once as kernel parameters), 0 when the networks differ
+ * further (each block then stages its own network's constants).  Results do not
+ * depend on it.  No counterpart in the reference, which runs one network per process. */
+int astrosim_ensemble_shared_constants(astrosim_ensemble* e, int* shared);
+
 int astrosim_ensemble_destroy(astrosim_ensemble* e);
 
 /* ------------------------------------------------------------------ serving

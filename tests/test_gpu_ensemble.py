@@ -27,6 +27,7 @@ def test_ensemble_matches_solo_runs(precision):
     cfgs = configs(precision, np.random.default_rng(3))
     with asg.Ensemble(cfgs) as ens:
         assert len(ens) == 7
+        assert ens.shared_constants()  # only seeds, sizes, drive rates and w_a2n differ
         ens.step(500)
         ens.step(500)  # 1000 steps = 100 windows: tuning windows, graph replays and a remainder
         got = []
@@ -45,6 +46,32 @@ def test_ensemble_matches_solo_runs(precision):
             solo = sim.summary()
             for k in ("spikes_total", "spikes_measured", "mean_ca", "active_astro", "engaged_astro"):
                 assert s[k] == solo[k], (i, k)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_ensemble_with_differing_constants_matches_solo_runs(precision):
+    """Networks whose biology differs beyond the per-network scalars take the
+    staged-constants window kernel; their results are still each solo run's."""
+    cfgs = [abi.default_config(n_total=n, seed=40 + i, pre_ms=10.0, sim_ms=60.0, precision=precision)
+            for i, n in enumerate((900, 2500, 1700))]
+    bios = [None, {"stp_U": 0.3, "SIC_th": 0.18}, {"exc_poiss_rate": 3100.0}]
+    with asg.Ensemble(cfgs, biology=bios) as ens:
+        assert not ens.shared_constants()
+        ens.step(700)
+        got = [({k: ens.state(i, k) for k in STATES}, ens.spike_counts(i)) for i in range(3)]
+    for i, (c, b) in enumerate(zip(cfgs, bios)):
+        with asg.Simulation(c, biology=b) as sim:
+            sim.step(700)
+            np.testing.assert_array_equal(got[i][1], sim.spike_counts())
+            for k in STATES:
+                np.testing.assert_array_equal(got[i][0][k], sim.state(k), err_msg=f"net {i} {k}")
+
+
+def test_ensemble_shares_constants_when_only_scalars_differ():
+    cfgs = [abi.default_config(n_total=n, seed=60 + i, pre_ms=0.0, sim_ms=20.0, precision="fp32")
+            for i, n in enumerate((700, 1400))]
+    with asg.Ensemble(cfgs, biology=[None, {"exc_poiss_rate": 3100.0, "inh_poiss_rate": 3100.0}]) as ens:
+        assert ens.shared_constants()  # the rates enter only through the per-network drive scalars
 
 
 def test_ensemble_rejects_mixed_precision_and_partial_windows():
