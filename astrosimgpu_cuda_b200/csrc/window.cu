@@ -35,10 +35,12 @@ __global__ void push_kernel(WinPtrs<R> w, u32 n_exc, u32 n_inh, u64 n_neurons, u
 }
 
 // ------------------------------------------------------------------ forward CSRs
+// One warp per target row, so that a row's entries are written by adjacent lanes.
 __global__ void edge_rows_kernel(const u32* rs, u32 n_rows, u32* row_of_edge) {
-    const u32 r = blockIdx.x * blockDim.x + threadIdx.x;
+    const u64 r = (static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     if (r >= n_rows) return;
-    for (u32 k = rs[r]; k < rs[r + 1]; ++k) row_of_edge[k] = r;
+    const u32 end = rs[r + 1];
+    for (u32 k = rs[r] + (threadIdx.x & 31u); k < end; k += 32) row_of_edge[k] = static_cast<u32>(r);
 }
 
 __global__ void iota_kernel(u32* v, u64 n) {
@@ -80,17 +82,36 @@ Status invert_csr(const DeviceCSR& c, u32 n_sources, DevBuf<u32>& rs, DevBuf<u32
         AS_CUDA(cudaMemsetAsync(rs.get(), 0, rs.bytes(), st));
         return Status::Ok();
     }
-    DevBuf<u32> row_of, idx_in, keys_out, idx_out;
+    DevBuf<u32> row_of, keys_out;
     AS_TRY(row_of.alloc(n));
-    AS_TRY(idx_in.alloc(n));
     AS_TRY(keys_out.alloc(n));
-    AS_TRY(idx_out.alloc(n));
-    edge_rows_kernel<<<ceil_div(c.n_targets, 256), 256, 0, st>>>(c.row_start.get(), c.n_targets, row_of.get());
-    iota_kernel<<<ceil_div(n, 256), 256, 0, st>>>(idx_in.get(), n);
+    edge_rows_kernel<<<ceil_div(static_cast<u64>(c.n_targets) * 32, 256), 256, 0, st>>>(c.row_start.get(), c.n_targets,
+                                                                                     row_of.get());
     AS_CUDA(cudaGetLastError());
     int end_bit = 1;
     while (end_bit < 32 && (1ull << end_bit) < static_cast<u64>(n_sources) + 1) ++end_bit;
     size_t tb = 0;
+    if (!pos) {
+        // Sorting the target rows themselves by source gives the forward lists
+        // directly (the same lists as the edge-index route below, without its index
+        // arrays and gather pass).
+        AS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, c.src.get(), keys_out.get(), row_of.get(), dst.get(), n,
+                                                0, end_bit, st));
+        DevBuf<unsigned char> tmp;
+        AS_TRY(tmp.alloc(tb));
+        AS_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), tb, c.src.get(), keys_out.get(), row_of.get(), dst.get(),
+                                                n, 0, end_bit, st));
+        lower_bound_rows_kernel<<<ceil_div(static_cast<u64>(n_sources) + 1, 256), 256, 0, st>>>(keys_out.get(), n,
+                                                                                              n_sources, rs.get());
+        AS_CUDA(cudaGetLastError());
+        AS_CUDA(cudaStreamSynchronize(st));
+        return Status::Ok();
+    }
+    DevBuf<u32> idx_in, idx_out;
+    AS_TRY(idx_in.alloc(n));
+    AS_TRY(idx_out.alloc(n));
+    iota_kernel<<<ceil_div(n, 256), 256, 0, st>>>(idx_in.get(), n);
+    AS_CUDA(cudaGetLastError());
     AS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, c.src.get(), keys_out.get(), idx_in.get(), idx_out.get(), n,
                                             0, end_bit, st));
     DevBuf<unsigned char> tmp;
@@ -100,7 +121,7 @@ Status invert_csr(const DeviceCSR& c, u32 n_sources, DevBuf<u32>& rs, DevBuf<u32
     lower_bound_rows_kernel<<<ceil_div(static_cast<u64>(n_sources) + 1, 256), 256, 0, st>>>(keys_out.get(), n,
                                                                                           n_sources, rs.get());
     gather_fwd_kernel<<<ceil_div(n, 256), 256, 0, st>>>(idx_out.get(), n, row_of.get(), c.row_start.get(), dst.get(),
-                                                        pos ? pos->get() : nullptr);
+                                                        pos->get());
     AS_CUDA(cudaGetLastError());
     AS_CUDA(cudaStreamSynchronize(st));
     return Status::Ok();
