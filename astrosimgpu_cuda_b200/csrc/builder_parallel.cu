@@ -55,6 +55,12 @@ constexpr unsigned long long kEmpty = ~0ull;
 constexpr u32 kNoSelf = 0xFFFFFFFFu;
 constexpr u32 kGroup = 64;  // chunks composed per group
 constexpr u32 kMaxDelta = 512;  // candidate entries (walkers) per chunk
+// A section with fewer than kTargetChunks chunks of its planned length runs with
+// shorter chunks, down to kMinChunkLen (4 x kMaxDelta): the table and orbit passes
+// walk one chunk per thread, position after position, so on small networks the
+// chunk length, not the network, sets their time.
+constexpr u32 kTargetChunks = 148 * 8;
+constexpr u32 kMinChunkLen = 2048;
 
 enum ErrBits : int {
     kErrCache = 1,     // a walk left the skip cache
@@ -473,6 +479,10 @@ struct SectionPlan {
 Status section_orbit(const SectionPlan& P, Sec s, u64 start, DevBuf<int>& err, DevBuf<u64>& orbit, u64* end,
                      cudaStream_t st) {
     u32 chunk_len = P.chunk_len, delta = P.delta;
+    {
+        const double draws = static_cast<double>(P.n_pres) * P.draws_per_pre;
+        while (chunk_len > kMinChunkLen && draws / chunk_len < kTargetChunks) chunk_len /= 2;
+    }
     double slack = 1.04;
     int K = 32;
     // Explicit pre starts kept per re-merge walk.  Walks rejoin after a median of 2

@@ -29,7 +29,18 @@ namespace astrosim {
 namespace {
 
 constexpr int kMaxTypes = 4;
-constexpr u32 kChunkNormals = 2048;  // normals per chunk (even)
+constexpr u32 kMaxChunkNormals = 2048;  // normals per chunk at most (every length is even)
+
+// Normals per chunk of a phase that budgets `budget` normals.  One thread scans each
+// chunk, one normal after the other, and one thread then composes the chunks, one
+// after the other; a step of either costs about the same, so the length follows the
+// square root of the budget: 64 for a few thousand normals, the 2048 cap from
+// about 4e6 on (the astrocyte phase of networks from N = 5e5 up).
+u32 chunk_normals(u64 budget) {
+    u32 c = 64;
+    while (c < kMaxChunkNormals && static_cast<u64>(c) * c < budget) c *= 2;
+    return c;
+}
 
 struct TypeSpec {
     double mean, sd, lo, hi;
@@ -41,6 +52,7 @@ struct Phase {
     int n_types;      // cycle length
     u64 n_units;      // draw_scaled calls in the phase
     u64 k_start;      // first normal index of the phase
+    u32 chunk;        // normals per chunk (chunk_normals)
 };
 
 // src/astrosim_fused.cu:210-216
@@ -95,7 +107,7 @@ struct ChunkResult {
     u32 accepts;   // completed units
     u8 exit_type;  // type index at the chunk end
     u8 tries;      // rejections of the unit in progress at the chunk end (capped)
-    u16 pad;
+    u16 lead;      // rejections before the chunk's first accept (the whole chunk if none)
 };
 
 // One thread per (chunk, entry type): run the automaton over the chunk.
@@ -105,14 +117,15 @@ __global__ void param_table_kernel(Phase ph, u64 seed, u32 n_chunks, ChunkResult
     const u32 chunk = gid / kMaxTypes;
     const int entry = gid % kMaxTypes;
     if (chunk >= n_chunks || entry >= ph.n_types) return;
-    const u64 k0 = ph.k_start + static_cast<u64>(chunk) * kChunkNormals;
+    const u64 k0 = ph.k_start + static_cast<u64>(chunk) * ph.chunk;
     int type = entry;
-    u32 acc = 0;
+    u32 acc = 0, lead = 0;
     int tries = 0;
-    for (u32 i = 0; i < kChunkNormals; ++i) {
+    for (u32 i = 0; i < ph.chunk; ++i) {
         const u64 k = k0 + i;
         const double z = normal_k(seed, k);
         if (accept(ph.t[type], k, z, tab, amb_k, amb_n, amb_cap)) {
+            if (acc == 0) lead = i;
             ++acc;
             type = type + 1 == ph.n_types ? 0 : type + 1;
             tries = 0;
@@ -124,20 +137,30 @@ __global__ void param_table_kernel(Phase ph, u64 seed, u32 n_chunks, ChunkResult
     r.accepts = acc;
     r.exit_type = static_cast<u8>(type);
     r.tries = static_cast<u8>(tries > 255 ? 255 : tries);
+    r.lead = static_cast<u16>(acc == 0 ? ph.chunk : lead);
     out[static_cast<u64>(chunk) * kMaxTypes + entry] = r;
 }
 
-// One thread composes the chunks in order.
+// One thread composes the chunks in order.  It also follows the run of rejections
+// of the unit in progress across chunk ends (the table scan sees runs inside a chunk).
 __global__ void param_compose_kernel(Phase ph, u32 n_chunks, const ChunkResult* tabs, u8* entry_type,
-                                     u64* unit_offset, u32* end_chunk) {
+                                     u64* unit_offset, u32* end_chunk, int* err) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     int type = 0;
     u64 units = 0;
+    u32 run = 0;
     u32 c = 0;
     for (; c < n_chunks; ++c) {
         entry_type[c] = static_cast<u8>(type);
         unit_offset[c] = units;
         const ChunkResult r = tabs[static_cast<u64>(c) * kMaxTypes + type];
+        if (r.accepts == 0) {
+            run += r.lead;
+        } else {
+            if (run + r.lead >= 200) *err = 1;
+            run = r.tries;
+        }
+        if (run >= 200) *err = 1;
         if (units + r.accepts >= ph.n_units) break;
         units += r.accepts;
         type = r.exit_type;
@@ -151,10 +174,10 @@ __global__ void param_emit_kernel(Phase ph, u64 seed, u32 n_chunks, const u8* en
     const u32 chunk = blockIdx.x * blockDim.x + threadIdx.x;
     const u32 last = *end_chunk;
     if (chunk >= n_chunks || chunk > last) return;
-    const u64 k0 = ph.k_start + static_cast<u64>(chunk) * kChunkNormals;
+    const u64 k0 = ph.k_start + static_cast<u64>(chunk) * ph.chunk;
     int type = entry_type[chunk];
     u64 unit = unit_offset[chunk];
-    for (u32 i = 0; i < kChunkNormals && unit < ph.n_units; ++i) {
+    for (u32 i = 0; i < ph.chunk && unit < ph.n_units; ++i) {
         const u64 k = k0 + i;
         const double z = normal_k(seed, k);
         if (accept(ph.t[type], k, z, tab, nullptr, nullptr, 0)) {
@@ -218,7 +241,8 @@ Status run_phase(Phase ph, u64 seed, double* const* dst_host, u64 n_cells, u64* 
     AS_TRY(amb_n.alloc(1));
     AS_TRY(err.alloc(1));
     for (int attempt = 0; attempt < 8; ++attempt) {
-        const u32 n_chunks = ceil_div(budget, kChunkNormals);
+        ph.chunk = chunk_normals(budget);
+        const u32 n_chunks = ceil_div(budget, ph.chunk);
         DevBuf<ChunkResult> tabs;
         DevBuf<u8> entry;
         DevBuf<u64> offs, kend;
@@ -290,11 +314,15 @@ Status run_phase(Phase ph, u64 seed, double* const* dst_host, u64 n_cells, u64* 
                 continue;
             }
         }
-        param_compose_kernel<<<1, 32, 0, st>>>(ph, n_chunks, tabs.get(), entry.get(), offs.get(), endc.get());
+        param_compose_kernel<<<1, 32, 0, st>>>(ph, n_chunks, tabs.get(), entry.get(), offs.get(), endc.get(),
+                                                err.get());
         AS_CUDA(cudaGetLastError());
         u32 hend = 0;
         AS_CUDA(cudaMemcpyAsync(&hend, endc.get(), sizeof(u32), cudaMemcpyDeviceToHost, st));
+        AS_CUDA(cudaMemcpyAsync(&herr, err.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
         AS_CUDA(cudaStreamSynchronize(st));
+        if (herr)
+            return make_error(ASTROSIM_ERR_UNSUPPORTED, "parameter stream with 200 consecutive rejections");
         if (hend >= n_chunks) {
             budget *= 2;  // the phase needed more normals than budgeted
             continue;
