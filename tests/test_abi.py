@@ -74,6 +74,9 @@ def test_null_and_bad_arguments_return_status(L):
     assert b"null" in L.astrosim_last_error()
     assert L.astrosim_summary(None, None) == abi.ERR_INVALID_ARG
     assert L.astrosim_destroy(None) == abi.OK
+    shared = C.c_int(7)
+    assert L.astrosim_ensemble_shared_constants(None, C.byref(shared)) == abi.ERR_INVALID_ARG
+    assert shared.value == 7
     h = C.c_void_p()
     cfg = abi.default_config()
     cfg.struct_size = 4
