@@ -91,7 +91,7 @@ def default_config(**overrides):
     cfg.seed = 1
     cfg.dt = 0.1
     cfg.substeps = 1
-    cfg.block = 128
+    cfg.block = 0  # autotuned; the reference launches 128-thread blocks (--block 128)
     cfg.pre_ms = 1000.0
     cfg.sim_ms = 5000.0
     cfg.w_n2a = math.nan

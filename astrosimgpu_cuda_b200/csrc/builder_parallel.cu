@@ -55,11 +55,12 @@ constexpr unsigned long long kEmpty = ~0ull;
 constexpr u32 kNoSelf = 0xFFFFFFFFu;
 constexpr u32 kGroup = 64;  // chunks composed per group
 constexpr u32 kMaxDelta = 512;  // candidate entries (walkers) per chunk
-// A section with fewer than kTargetChunks chunks of its planned length runs with
-// shorter chunks, down to kMinChunkLen (4 x kMaxDelta): the table and orbit passes
-// walk one chunk per thread, position after position, so on small networks the
-// chunk length, not the network, sets their time.
-constexpr u32 kTargetChunks = 148 * 8;
+// A section with fewer than target_chunks() (8 per SM) chunks of its planned length
+// runs with shorter chunks, down to kMinChunkLen (4 x kMaxDelta): the table and orbit
+// passes walk one chunk per thread, position after position, so on small networks
+// the chunk length, not the network, sets their time.  The chunking never changes
+// the result, only how the walk is split.
+inline u32 target_chunks() { return sm_count() * 8; }
 constexpr u32 kMinChunkLen = 2048;
 
 enum ErrBits : int {
@@ -481,7 +482,7 @@ Status section_orbit(const SectionPlan& P, Sec s, u64 start, DevBuf<int>& err, D
     u32 chunk_len = P.chunk_len, delta = P.delta;
     {
         const double draws = static_cast<double>(P.n_pres) * P.draws_per_pre;
-        while (chunk_len > kMinChunkLen && draws / chunk_len < kTargetChunks) chunk_len /= 2;
+        while (chunk_len > kMinChunkLen && draws / chunk_len < target_chunks()) chunk_len /= 2;
     }
     double slack = 1.04;
     int K = 32;
@@ -739,7 +740,7 @@ Status build_parallel(const Sizes& sz, u64 seed, u64 c0, Network& net, cudaStrea
         AS_TRY(amb_val.alloc(amb_cap));
         AS_TRY(amb_n.alloc_zero(1, st));
         AmbiguityLog amb{amb_pos.get(), amb_val.get(), amb_n.get(), amb_cap};
-        skip_cache_kernel<<<148 * 16, 256, 0, st>>>(seed, L, pools_end, cache_len, cache.get(), amb);
+        skip_cache_kernel<<<sm_count() * 16, 256, 0, st>>>(seed, L, pools_end, cache_len, cache.get(), amb);
         AS_CUDA(cudaGetLastError());
         unsigned n_amb = 0;
         AS_TRY(to_host(&n_amb, amb_n.get(), 1, st));

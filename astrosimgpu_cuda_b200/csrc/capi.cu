@@ -10,6 +10,8 @@
 
 #include <mutex>
 
+#include <cuda.h>
+
 #include "../../include/astrosim.h"
 #include "biology.cuh"
 #include "ensemble.cuh"
@@ -69,7 +71,7 @@ void astrosim_config_default(astrosim_config* cfg) {
     cfg->seed = 1;
     cfg->dt = 0.1;
     cfg->substeps = 1;
-    cfg->block = 128;
+    cfg->block = 0;           // the reference launches 128-thread blocks; 0 = autotuned
     cfg->pre_ms = 1000.0;
     cfg->sim_ms = 5000.0;
     cfg->w_n2a = std::nan("");
@@ -366,8 +368,44 @@ static_assert(sizeof(astrosim_astro_totals) == sizeof(astrosim::AstroTotals), "t
 static __device__ __align__(256) astrosim::AstroPartial g_noalloc_partials[kNoAllocPartials];
 
 constexpr int kMaxDevices = 128;
+
+// The scratch address belongs to one CUDA context: after cudaDeviceReset (or any
+// new primary context) the device image is loaded again, possibly elsewhere.  The
+// cache is keyed by the driver's context id, which is unique for the life of the
+// process (a context's address can be reused; its id is not).  The two driver
+// calls are fetched through the runtime, so the library needs no driver link.
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+struct NoAllocSlot {
+    unsigned long long ctx_id = 0;
+    astrosim::AstroPartial* addr = nullptr;
+};
 std::mutex g_noalloc_mu;
-astrosim::AstroPartial* g_noalloc_addr[kMaxDevices] = {};
+NoAllocSlot g_noalloc_slot[kMaxDevices];
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+CtxGetIdFn g_ctx_get_id = nullptr;
+
+// Id of the current context (made current by a runtime call first); 0 on failure.
+unsigned long long current_context_id() {
+    if (!g_ctx_get_current || !g_ctx_get_id) {
+        void* f1 = nullptr;
+        void* f2 = nullptr;
+        cudaDriverEntryPointQueryResult q1{}, q2{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) != cudaSuccess ||
+            cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) != cudaSuccess ||
+            q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess || !f1 || !f2) {
+            cudaGetLastError();
+            return 0;
+        }
+        g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(f1);
+        g_ctx_get_id = reinterpret_cast<CtxGetIdFn>(f2);
+    }
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (g_ctx_get_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+    if (g_ctx_get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
 
 }  // namespace
 
@@ -387,18 +425,26 @@ extern "C" int astrosim_astro_totals_noalloc(const double* ca, const unsigned ch
     if (dev < 0 || dev >= kMaxDevices) return fail(ASTROSIM_ERR_INVALID_ARG, "device ordinal too large");
     astrosim::AstroPartial* scratch = nullptr;
     {
-        // once per device, with that device current: the device address of the scratch
+        // once per device context, with that device current: the device address of
+        // the scratch.  Before the first runtime call of a thread no context may be
+        // current (id 0); cudaGetSymbolAddress then creates the device's primary
+        // context, and the id is read again after it.
         std::lock_guard<std::mutex> lock(g_noalloc_mu);
-        if (!g_noalloc_addr[dev]) {
+        unsigned long long ctx = current_context_id();
+        NoAllocSlot& slot = g_noalloc_slot[dev];
+        if (ctx == 0 || !slot.addr || slot.ctx_id != ctx) {
             void* p = nullptr;
             e = cudaGetSymbolAddress(&p, g_noalloc_partials);
-            if (e != cudaSuccess || !p) {
+            ctx = current_context_id();
+            if (e != cudaSuccess || !p || ctx == 0) {
                 cudaGetLastError();
+                slot = NoAllocSlot{};
                 return fail(ASTROSIM_ERR_CUDA, "cudaGetSymbolAddress of the no-alloc scratch failed");
             }
-            g_noalloc_addr[dev] = static_cast<astrosim::AstroPartial*>(p);
+            slot.addr = static_cast<astrosim::AstroPartial*>(p);
+            slot.ctx_id = ctx;
         }
-        scratch = g_noalloc_addr[dev];
+        scratch = slot.addr;
     }
     return guarded([&] {
         return astrosim::astro_totals(ca, engaged, n_astro, sic_th, scratch,

@@ -31,7 +31,7 @@ int die(const char* what) {
 void print_help() {
     std::printf(
         "astrosim --n N_total [--seed S] [--dt 0.1] [--substeps 1] "
-        "[--pre-ms 1000] [--sim-ms 5000] [--block 128]\n"
+        "[--pre-ms 1000] [--sim-ms 5000] [--block N]\n"
         "         [--w-n2a W] [--w-a2n W] [--no-stp] [--dump-edges PATH]\n"
         "         [--precision fp64|fp32] [--device N] [--biology FILE.json]\n"
         "N_total is split by the fixed-in-degree scaling law: N_E=0.8*N, N_I=0.2*N,\n"
@@ -39,6 +39,8 @@ void print_help() {
         "astrocyte->neuron coupling weight (default 0.2 / 1.0); 0 disconnects that\n"
         "direction.  --no-stp disables Tsodyks-Markram short-term plasticity.\n"
         "--dump-edges PATH writes the network as type,source,target CSV and exits.\n"
+        "--block N sets the CUDA block size of the cell kernels (the reference uses\n"
+        "128); without it the autotuner picks the block size and occupancy.\n"
         "--precision fp32 runs RK4 stages in float with double accumulators.\n"
         "--biology FILE reads a JSON object of biology constants to override, e.g.\n"
         "{\"exc_poiss_rate\": 3000, \"stp_U\": 0.4}; the flags above apply on top.\n"

@@ -193,4 +193,23 @@ inline void give_stream(int device, cudaStream_t s) {
 
 inline unsigned ceil_div(uint64_t a, uint64_t b) { return static_cast<unsigned>((a + b - 1) / b); }
 
+// Streaming multiprocessors of the current device (cudaDevAttrMultiProcessorCount),
+// read once per device; grids of persistent and grid-stride kernels are sized by it.
+inline unsigned sm_count() {
+    static unsigned cached[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) {
+        cudaGetLastError();
+        return 148;
+    }
+    if (dev < 64 && cached[dev]) return cached[dev];
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) {
+        cudaGetLastError();
+        n = 148;  // B200
+    }
+    if (dev < 64) cached[dev] = static_cast<unsigned>(n);  // idempotent: every writer stores the same value
+    return static_cast<unsigned>(n);
+}
+
 }  // namespace astrosim

@@ -181,7 +181,7 @@ Status push_phase(ShardSim& s, i64 k) {
     const RunConsts& rc = sim.consts();
     WindowState& ws = *sim.window_state();
     WinPtrs<R> w = win_ptrs<R>(ws, rc);
-    const u32 blocks = std::max<u32>(1, std::min<u32>(148 * 8, ceil_div(ws.push_limit, 8)));
+    const u32 blocks = std::max<u32>(1, std::min<u32>(sm_count() * 8, ceil_div(ws.push_limit, 8)));
     shard_push_kernel<R><<<blocks, 256, 0, sim.stream()>>>(w, rc.n_exc, sim.network().sz.n_inh, rc.n_neurons,
                                                            rc.n_astro, static_cast<int>(k & 1), s.plan.n_lo,
                                                            s.plan.n_hi, s.plan.a_lo, s.plan.a_hi);

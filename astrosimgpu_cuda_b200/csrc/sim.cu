@@ -285,7 +285,7 @@ Status Simulation::ensure_counts(i64 steps) {
 Status Simulation::launch_steps(i64 first, i64 count) {
     if (windowed_) {
         const i64 mark = pre_steps_ == 0 ? 0 : pre_steps_ - 1;
-        return window_launch(rc_, st_, net_, fp32_, *win_, cfg_.raster_steps, mark, first, count, stream_, block_);
+        return window_launch(rc_, st_, net_, fp32_, *win_, cfg_.raster_steps, mark, first, count, stream_, cfg_.block);
     }
     const u32 astro_blocks = ceil_div(rc_.n_astro, block_);
     const u32 neuron_blocks = ceil_div(rc_.n_neurons, block_);

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <map>
+#include <tuple>
 #include <mutex>
 #include <type_traits>
 #include <utility>
@@ -17,13 +18,15 @@ namespace astrosim {
 
 namespace {
 
-// MinBlocks is the launch-bounds occupancy target: the autotuner (window_launch)
-// times the instantiated values on the first windows of a run and keeps the fastest.
-// The per-cell arithmetic is the same in every instantiation.
-template <typename R, int MinBlocks>
-__global__ void __launch_bounds__(128, MinBlocks) window_kernel(RunConsts rc, StepPtrs<R> p, WinPtrs<R> w,
-                                                                i64 win_start, int s_begin, int s_end, int buf,
-                                                                i64 mark, u32 astro_blocks) {
+// Block and MinBlocks are the block size and the launch-bounds occupancy target
+// (resident blocks per SM): the autotuner (window_launch) times the instantiated
+// pairs on the first windows of a run and keeps the fastest.  The per-cell
+// arithmetic is the same in every instantiation; the kernel indexes cells by
+// blockDim.x, so Block = 1024 with MinBlocks = 1 serves any other block size.
+template <typename R, int Block, int MinBlocks>
+__global__ void __launch_bounds__(Block, MinBlocks) window_kernel(RunConsts rc, StepPtrs<R> p, WinPtrs<R> w,
+                                                                  i64 win_start, int s_begin, int s_end, int buf,
+                                                                  i64 mark, u32 astro_blocks) {
     const bool astro = blockIdx.x < astro_blocks;
     window_cells<R>(rc, net_scalars(rc), p, w, win_start, s_begin, s_end, buf, mark, astro ? blockIdx.x : blockIdx.x - astro_blocks,
                     astro);
@@ -159,51 +162,110 @@ Status window_setup(const RunConsts& rc, Network& net, bool fp32, WindowState& w
 
 namespace {
 
-// Launch-bounds variants the autotuner chooses from (minimum resident blocks of 128
-// threads per SM): more blocks trade registers (and a few spills) for occupancy.
-constexpr int kVariantsF32[] = {6, 8, 4};
-constexpr int kVariantsF64[] = {4, 5, 3};
-constexpr int kNumVariants = 3;
+// Variants the autotuner chooses from: (block size, minimum resident blocks per SM).
+// Each block size comes with three occupancy targets (the same threads per SM as
+// the 128-thread entries), trading registers (and a few spills) for occupancy.
+struct Variant {
+    int block, min_blocks;
+};
+constexpr Variant kVariantsF32[] = {{128, 6}, {128, 8}, {128, 4}, {64, 12}, {64, 16}, {64, 8},
+                                    {256, 3}, {256, 4}, {256, 2}};
+constexpr Variant kVariantsF64[] = {{128, 4}, {128, 5}, {128, 3}, {64, 8}, {64, 10}, {64, 6},
+                                    {256, 2}, {256, 3}, {256, 1}};
+constexpr int kNumVariants = 9;
+constexpr int kVariantsPerBlock = 3;
 constexpr int kTuneRounds = 2;
+static_assert(sizeof(kVariantsF32) / sizeof(Variant) == kNumVariants, "variant table");
+static_assert(sizeof(kVariantsF64) / sizeof(Variant) == kNumVariants, "variant table");
+
+// The variants a run may use: every entry for block 0 (the autotuned choice), the
+// three entries of a tuned block size, or the generic instantiation (index -1) for
+// any other requested block size.
+void variant_range(int block, int* first, int* count) {
+    for (int b = 0; b < kNumVariants / kVariantsPerBlock; ++b)
+        if (kVariantsF32[b * kVariantsPerBlock].block == block) {
+            *first = b * kVariantsPerBlock;
+            *count = kVariantsPerBlock;
+            return;
+        }
+    if (block == 0) {
+        *first = 0;
+        *count = kNumVariants;
+        return;
+    }
+    *first = -1;
+    *count = 0;
+}
 
 std::mutex g_tune_mu;
-std::map<std::pair<int, int>, int> g_tuned;  // (precision, log2 size bucket) -> variant
+std::map<std::tuple<int, int, int>, int> g_tuned;  // (precision, log2 size bucket, requested block) -> variant
 
+template <typename R, int B, int M>
+void launch_one(u32 cells_astro, u32 cells_neuron, cudaStream_t st, const RunConsts& rc, const StepPtrs<R>& p,
+                const WinPtrs<R>& w, i64 start, int s0, int s1, int buf, i64 mark, int block) {
+    const u32 astro_blocks = ceil_div(cells_astro, block);
+    const u32 grid = astro_blocks + ceil_div(cells_neuron, block);
+    window_kernel<R, B, M><<<grid, block, 0, st>>>(rc, p, w, start, s0, s1, buf, mark, astro_blocks);
+}
+
+// Launches variant `variant` (an index into the table; -1 = the generic kernel at
+// `block` threads).
 template <typename R>
-void launch_window(int variant, u32 grid, cudaStream_t st, const RunConsts& rc, const StepPtrs<R>& p,
-                   const WinPtrs<R>& w, i64 start, int s0, int s1, int buf, i64 mark, u32 astro_blocks) {
+void launch_window(int variant, int block, cudaStream_t st, const RunConsts& rc, const StepPtrs<R>& p,
+                   const WinPtrs<R>& w, i64 start, int s0, int s1, int buf, i64 mark) {
     constexpr bool f32 = std::is_same<R, float>::value;
+    const u32 nA = rc.n_astro, nN = rc.n_neurons;
+#define AS_WIN(B, M) launch_one<R, B, M>(nA, nN, st, rc, p, w, start, s0, s1, buf, mark, B)
+    if (variant < 0) {
+        launch_one<R, 1024, 1>(nA, nN, st, rc, p, w, start, s0, s1, buf, mark, block);
+        return;
+    }
+    const Variant v = f32 ? kVariantsF32[variant] : kVariantsF64[variant];
     if constexpr (f32) {
-        switch (kVariantsF32[variant]) {
-            case 4: window_kernel<R, 4><<<grid, 128, 0, st>>>(rc, p, w, start, s0, s1, buf, mark, astro_blocks); break;
-            case 8: window_kernel<R, 8><<<grid, 128, 0, st>>>(rc, p, w, start, s0, s1, buf, mark, astro_blocks); break;
-            default: window_kernel<R, 6><<<grid, 128, 0, st>>>(rc, p, w, start, s0, s1, buf, mark, astro_blocks); break;
+        switch (v.block * 100 + v.min_blocks) {
+            case 12804: AS_WIN(128, 4); break;
+            case 12808: AS_WIN(128, 8); break;
+            case 6412: AS_WIN(64, 12); break;
+            case 6416: AS_WIN(64, 16); break;
+            case 6408: AS_WIN(64, 8); break;
+            case 25603: AS_WIN(256, 3); break;
+            case 25604: AS_WIN(256, 4); break;
+            case 25602: AS_WIN(256, 2); break;
+            default: AS_WIN(128, 6); break;
         }
     } else {
-        switch (kVariantsF64[variant]) {
-            case 3: window_kernel<R, 3><<<grid, 128, 0, st>>>(rc, p, w, start, s0, s1, buf, mark, astro_blocks); break;
-            case 5: window_kernel<R, 5><<<grid, 128, 0, st>>>(rc, p, w, start, s0, s1, buf, mark, astro_blocks); break;
-            default: window_kernel<R, 4><<<grid, 128, 0, st>>>(rc, p, w, start, s0, s1, buf, mark, astro_blocks); break;
+        switch (v.block * 100 + v.min_blocks) {
+            case 12803: AS_WIN(128, 3); break;
+            case 12805: AS_WIN(128, 5); break;
+            case 6408: AS_WIN(64, 8); break;
+            case 6410: AS_WIN(64, 10); break;
+            case 6406: AS_WIN(64, 6); break;
+            case 25602: AS_WIN(256, 2); break;
+            case 25603: AS_WIN(256, 3); break;
+            case 25601: AS_WIN(256, 1); break;
+            default: AS_WIN(128, 4); break;
         }
     }
+#undef AS_WIN
 }
 
 template <typename R>
 Status launch_impl(const RunConsts& rc, StateBuffers& sb, Network& net, WindowState& ws, i64 raster_steps, i64 mark,
-                   i64 first, i64 count, cudaStream_t st) {
+                   i64 first, i64 count, cudaStream_t st, int block) {
     constexpr bool f32 = std::is_same<R, float>::value;
     StepPtrs<R> p = make_ptrs<R>(sb, net, rc, raster_steps);
     WinPtrs<R> w = win_ptrs<R>(ws, rc);
-    const u32 astro_blocks = ceil_div(rc.n_astro, 128);
-    const u32 neuron_blocks = ceil_div(rc.n_neurons, 128);
     const int W = ws.W;
-    const u32 push_blocks = std::max<u32>(1, std::min<u32>(148 * 8, ceil_div(ws.push_limit, 8)));
+    const u32 push_blocks = std::max<u32>(1, std::min<u32>(sm_count() * 8, ceil_div(ws.push_limit, 8)));
+    int v_first = 0, v_count = 0;
+    variant_range(block, &v_first, &v_count);
+    if (v_first < 0) ws.variant = -2;  // a block size outside the table: the generic kernel, nothing to tune
     int bucket = 0;
     while ((1ull << bucket) < rc.n_neurons) ++bucket;
-    const std::pair<int, int> key{f32 ? 1 : 0, bucket};
-    if (ws.variant < 0) {
+    const std::tuple<int, int, int> key{f32 ? 1 : 0, bucket, block};
+    if (ws.variant == -1) {
         if (const char* env = std::getenv("ASTROSIM_WINDOW_VARIANT")) {
-            ws.variant = std::min(kNumVariants - 1, std::max(0, std::atoi(env)));
+            ws.variant = v_first + std::min(v_count - 1, std::max(0, std::atoi(env)));
         } else {
             std::lock_guard<std::mutex> lock(g_tune_mu);
             auto it = g_tuned.find(key);
@@ -217,24 +279,26 @@ Status launch_impl(const RunConsts& rc, StateBuffers& sb, Network& net, WindowSt
         const int s0 = static_cast<int>(t - k * W);
         const int s1 = static_cast<int>(std::min<i64>(W, end - k * W));
         const int buf = static_cast<int>(k & 1);
-        const bool tuning = ws.variant < 0 && s0 == 0 && s1 == W;
-        const int v = ws.variant >= 0 ? ws.variant : (tuning ? ws.tune_step % kNumVariants : 0);
+        const bool tuning = ws.variant == -1 && s0 == 0 && s1 == W;
+        int v = ws.variant >= 0 ? ws.variant : (tuning ? v_first + ws.tune_step % v_count : v_first);
+        if (ws.variant == -2) v = -1;
         if (tuning && !ws.tune_ev[0]) {  // made on the first tuned window only
             AS_CUDA(cudaEventCreate(&ws.tune_ev[0]));
             AS_CUDA(cudaEventCreate(&ws.tune_ev[1]));
         }
         if (tuning) AS_CUDA(cudaEventRecord(ws.tune_ev[0], st));
-        launch_window<R>(v, astro_blocks + neuron_blocks, st, rc, p, w, k * W, s0, s1, buf, mark, astro_blocks);
+        launch_window<R>(v, block, st, rc, p, w, k * W, s0, s1, buf, mark);
         AS_CUDA(cudaGetLastError());
         if (tuning) {
             AS_CUDA(cudaEventRecord(ws.tune_ev[1], st));
             AS_CUDA(cudaEventSynchronize(ws.tune_ev[1]));
             float ms = 0.f;
             AS_CUDA(cudaEventElapsedTime(&ms, ws.tune_ev[0], ws.tune_ev[1]));
-            ws.tune_ms[v] = std::min(ws.tune_ms[v], ms);  // min over rounds: the first launch also loads the kernel
-            if (++ws.tune_step == kNumVariants * kTuneRounds) {
-                int best = 0;
-                for (int i = 1; i < kNumVariants; ++i)
+            float& slot = ws.tune_ms[v];
+            slot = std::min(slot, ms);  // min over rounds: the first launch also loads the kernel
+            if (++ws.tune_step == v_count * kTuneRounds) {
+                int best = v_first;
+                for (int i = v_first + 1; i < v_first + v_count; ++i)
                     if (ws.tune_ms[i] < ws.tune_ms[best]) best = i;
                 ws.variant = best;
                 std::lock_guard<std::mutex> lock(g_tune_mu);
@@ -253,9 +317,8 @@ Status launch_impl(const RunConsts& rc, StateBuffers& sb, Network& net, WindowSt
 
 Status window_launch(const RunConsts& rc, StateBuffers& sb, Network& net, bool fp32, WindowState& ws,
                      i64 raster_steps, i64 mark_step, i64 first, i64 count, cudaStream_t st, int block) {
-    (void)block;
-    if (fp32) return launch_impl<float>(rc, sb, net, ws, raster_steps, mark_step, first, count, st);
-    return launch_impl<double>(rc, sb, net, ws, raster_steps, mark_step, first, count, st);
+    if (fp32) return launch_impl<float>(rc, sb, net, ws, raster_steps, mark_step, first, count, st, block);
+    return launch_impl<double>(rc, sb, net, ws, raster_steps, mark_step, first, count, st, block);
 }
 
 }  // namespace astrosim

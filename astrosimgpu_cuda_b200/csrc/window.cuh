@@ -53,10 +53,12 @@ struct WindowState {
     DevBuf<unsigned char> sic_win;            // [2][n_astro][W] real
     DevBuf<u32> astro_active;                 // [2][ceil(n_astro / 32)]
     DevBuf<int> mode;                         // [2]: 0 push, 1 pull
-    // autotuner: launch-bounds variant of window_kernel (-1 while timing the candidates)
+    // autotuner: (block size, launch bounds) variant of window_kernel, an index into
+    // its table; -1 while timing the candidates, -2 for the generic kernel (a block
+    // size outside the table, nothing to tune)
     int variant = -1;
     int tune_step = 0;
-    float tune_ms[4] = {1e30f, 1e30f, 1e30f, 1e30f};
+    float tune_ms[9] = {1e30f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f};
     cudaEvent_t tune_ev[2] = {nullptr, nullptr};
     ~WindowState() {
         if (tune_ev[0]) cudaEventDestroy(tune_ev[0]);
@@ -66,7 +68,8 @@ struct WindowState {
 
 Status window_setup(const RunConsts& rc, Network& net, bool fp32, WindowState& ws, cudaStream_t st);
 
-// Advances steps [first, first + count) with windows of ws.W steps.
+// Advances steps [first, first + count) with windows of ws.W steps.  `block` is the
+// window kernel's block size (a multiple of 32); 0 lets the autotuner choose it.
 Status window_launch(const RunConsts& rc, StateBuffers& sb, Network& net, bool fp32, WindowState& ws,
                      i64 raster_steps, i64 mark_step, i64 first, i64 count, cudaStream_t st, int block);
 

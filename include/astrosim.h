@@ -56,7 +56,11 @@ typedef struct astrosim_config {
     uint64_t seed;          /* --seed */
     double dt;              /* --dt, ms */
     int32_t substeps;       /* --substeps: RK4 substeps per time step */
-    int32_t block;          /* --block: CUDA block size for the cell kernels; 0 = autotuned choice */
+    int32_t block;          /* --block: CUDA block size of the cell kernels (a multiple of 32 in [32, 1024];
+                               the reference's default is 128).  0 (the default here) = the autotuner
+                               times block sizes 64/128/256 with three occupancy targets each on
+                               the first windows and keeps the fastest; a given size is used as is
+                               (64/128/256 still tune their occupancy target) */
     double pre_ms;          /* --pre-ms: discarded transient */
     double sim_ms;          /* --sim-ms: recorded window */
     double w_n2a;           /* --w-n2a: neuron->astrocyte weight; NaN keeps the default 0.2 */
@@ -375,7 +379,9 @@ typedef struct astrosim_astro_totals {
  * inputs return ASTROSIM_ERR_INVALID_ARG.
  *
  * The first call on a device (with that device current) looks up the scratch
- * address once; make that first call before any stream capture.  All calls share
+ * address once per CUDA context: again after cudaDeviceReset or any other change
+ * of the device's context, which can move the device image.  Make the first call
+ * in each context before any stream capture.  All calls share
  * the one scratch array: calls that may overlap on the GPU (different streams,
  * or different host threads) race and must be serialised by the caller.  Each
  * call writes every partial it reads, so nothing left by an earlier call leaks

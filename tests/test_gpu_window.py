@@ -55,11 +55,19 @@ def test_windowed_dt_quarter_ms(monkeypatch):
 
 @pytest.mark.parametrize("precision", ["fp32", "fp64"])
 def test_every_launch_variant_is_bit_identical(monkeypatch, precision):
+    """Every (block size, occupancy target) pair the autotuner may pick (block 0:
+    nine variants over 64/128/256 threads), a fixed tuned size (64: its three
+    variants) and block sizes outside the table (96, 512: the generic kernel) give
+    the per-step path's results bit for bit."""
     kw = dict(n_total=4000, seed=5, pre_ms=20, sim_ms=60, precision=precision)
     ref = run(monkeypatch, "plain", None, (800,), **kw)
-    for v in (0, 1, 2):
-        monkeypatch.setenv("ASTROSIM_WINDOW_VARIANT", str(v))
-        got = run(monkeypatch, "auto", None, (13, 787), **kw)
+    cases = [(0, v) for v in range(9)] + [(64, v) for v in range(3)] + [(96, None), (512, None), (256, None)]
+    for block, v in cases:
+        if v is None:
+            monkeypatch.delenv("ASTROSIM_WINDOW_VARIANT", raising=False)
+        else:
+            monkeypatch.setenv("ASTROSIM_WINDOW_VARIANT", str(v))
+        got = run(monkeypatch, "auto", None, (13, 787), block=block, **kw)
         for k in STATES + ("counts",):
-            np.testing.assert_array_equal(got[k], ref[k], err_msg=f"{k} variant {v}")
-    monkeypatch.delenv("ASTROSIM_WINDOW_VARIANT")
+            np.testing.assert_array_equal(got[k], ref[k], err_msg=f"{k} block {block} variant {v}")
+    monkeypatch.delenv("ASTROSIM_WINDOW_VARIANT", raising=False)
