@@ -40,15 +40,22 @@ def build(jobs=8):
     subprocess.run(["make", "-s", "-C", HERE, f"-j{jobs}"], check=True)
 
 
+def library_path():
+    """The library this process uses: lib/libastrosim_b200.so, or the path in
+    ASTROSIM_LIBRARY (e.g. the FP32 measurement build lib/libastrosim_b200_fp32ieee.so)."""
+    return os.environ.get("ASTROSIM_LIBRARY") or LIB_PATH
+
+
 def lib():
     """Loads the CUDA library; raises if it has not been built."""
     global _lib
     if _lib is not None:
         return _lib
-    if not os.path.exists(LIB_PATH):
-        raise ImportError(f"{LIB_PATH} is missing: build it with `make -C {HERE}` "
+    path = library_path()
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with `make -C {HERE}` "
                           "(the simulator has no CPU fallback)")
-    L = C.CDLL(LIB_PATH)
+    L = C.CDLL(path)
     P = C.c_void_p
     u32p = C.POINTER(C.c_uint32)
     L.astrosim_config_default.argtypes = [C.POINTER(abi.Config)]

@@ -295,6 +295,18 @@ inline int delay_to_steps(double delay_ms, double dt) {  // src/astrosim_fused.c
 
 // ------------------------------------------------------------------ device arithmetic
 #ifdef __CUDACC__
+#ifdef ASTROSIM_FP32_IEEE
+// Measurement build of the FP32 form (make fp32ieee): every float function below
+// is CUDA's IEEE-conformant one (expf, logf, sqrtf, cosf, correctly rounded
+// division) and the noise uniforms keep 53 bits, so that comparing it with the
+// default build separates what the hardware approximations cost in agreement with
+// FP64 from what float stages cost.  The default build is the product.
+__device__ __forceinline__ float exp_fast(float x) { return expf(x); }
+__device__ __forceinline__ float log_fast(float x) { return logf(x); }
+__device__ __forceinline__ float div_fast(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ float sqrt_ftz(float x) { return __fsqrt_rn(x); }
+__device__ __forceinline__ float cos_ftz(float x) { return cosf(x); }
+#else
 // Hardware approximations of the FP32 form, denormals flushed to zero:
 // exp(x) = 2^(x log2 e), log(x) = log2(x) ln 2, a / b = a * (1 / b).
 __device__ __forceinline__ float ex2_ftz(float x) {
@@ -327,6 +339,7 @@ constexpr float kLn2 = 0.69314718055994530942f;    // ln(2)
 __device__ __forceinline__ float exp_fast(float x) { return ex2_ftz(x * kLog2E); }
 __device__ __forceinline__ float log_fast(float x) { return lg2_ftz(x) * kLn2; }
 __device__ __forceinline__ float div_fast(float a, float b) { return a * rcp_ftz(b); }
+#endif  // ASTROSIM_FP32_IEEE
 
 // x / y rounded to nearest, for a divisor whose reciprocal ry = RN(1 / y) is known.
 // q0 = RN(x ry) is within 1.5 ulp of x / y; one correction q1 = RN(q0 + (x - q0 y) ry)
@@ -391,30 +404,53 @@ __device__ __forceinline__ void neuron_rhs(const NeuronK& p, double V, double w,
 __device__ __forceinline__ void neuron_rhs(const NeuronK& p, float V, float w, float g_ex, float g_in, float I_ext,
                                            float& dV, float& dw) {
     const float Vc = V < p.f_V_peak ? V : p.f_V_peak;
+#ifdef ASTROSIM_FP32_IEEE
+    // the FP64 path's operations in float: divisions, not reciprocal multiplies
+    const float DT = static_cast<float>(p.Delta_T);
+    const float I_spike = p.f_g_L * DT * exp_fast((Vc - p.f_V_th) / DT);
+    const float I_syn_ex = g_ex * (Vc - p.f_E_ex);
+    const float I_syn_in = g_in * (Vc - p.f_E_in);
+    dV = (-p.f_g_L * (Vc - p.f_E_L) + I_spike - I_syn_ex - I_syn_in - w + p.f_I_e + I_ext) / static_cast<float>(p.C_m);
+    dw = (p.f_a * (Vc - p.f_E_L) - w) / static_cast<float>(p.tau_w);
+#else
     const float I_spike = p.f_gL_DT * exp_fast((Vc - p.f_V_th) * p.f_inv_DT);
     const float I_syn_ex = g_ex * (Vc - p.f_E_ex);
     const float I_syn_in = g_in * (Vc - p.f_E_in);
     dV = (-p.f_g_L * (Vc - p.f_E_L) + I_spike - I_syn_ex - I_syn_in - w + p.f_I_e + I_ext) * p.f_inv_Cm;
     dw = (p.f_a * (Vc - p.f_E_L) - w) * p.f_inv_tauw;
+#endif
 }
 
 // The FP32 form of the Li-Rinzel right-hand side (see astro_rhs).
-__device__ __forceinline__ void astro_rhs_fast(const AstroK& c, float Ca_tot, float IP3_0, float inv_tau_IP3,
+__device__ __forceinline__ void astro_rhs_fast(const AstroK& c, float Ca_tot, float IP3_0, float tau_IP3, float inv_tau_IP3,
                                                float Ca, float IP3, float h, float noise, float& dCa, float& dIP3,
                                                float& dh) {
+#ifdef ASTROSIM_FP32_IEEE
+    const float Ca_ER = (Ca_tot - Ca) / static_cast<float>(c.ratio_ER_cyt);
+#else
     const float Ca_ER = (Ca_tot - Ca) * c.f_inv_ratio;
+#endif
     const float m_inf = div_fast(IP3, IP3 + c.f_Kd_IP3_1);
     const float n_inf = div_fast(Ca, Ca + c.f_Kd_act);
     const float m3 = m_inf * m_inf * m_inf;
     const float n3 = n_inf * n_inf * n_inf;
     const float h3 = h * h * h;
+#ifdef ASTROSIM_FP32_IEEE
+    const float J_channel =
+        static_cast<float>(c.ratio_ER_cyt) * static_cast<float>(c.rate_IP3R) * m3 * n3 * h3 * (Ca_ER - Ca);
+#else
     const float J_channel = c.f_ratio_rate_IP3R * m3 * n3 * h3 * (Ca_ER - Ca);
+#endif
     const float J_pump = div_fast(c.f_rate_SERCA * Ca * Ca, c.f_Km2 + Ca * Ca);
     const float J_leak = c.f_ratio_rate_L * (Ca_ER - Ca);
     const float alpha_h = div_fast(c.f_k_Kd_inh * (IP3 + c.f_Kd_IP3_1), IP3 + c.f_Kd_IP3_2);
     const float beta_h = c.f_k_IP3R * Ca;
     dCa = J_channel - J_pump + J_leak + noise;
+#ifdef ASTROSIM_FP32_IEEE
+    dIP3 = (IP3_0 - IP3) / tau_IP3;
+#else
     dIP3 = (IP3_0 - IP3) * inv_tau_IP3;
+#endif
     dh = alpha_h * (1.0f - h) - beta_h * h;
 }
 
@@ -428,11 +464,20 @@ __host__ __device__ __forceinline__ float as_r<float>(double, float f) { return 
 
 // Box-Muller in float from one stream (counters 0 and 1): the noise draws of the FP32 form.
 __device__ __forceinline__ float normal_fast(u64 base) {
+#ifdef ASTROSIM_FP32_IEEE
+    // the FP64 path's 53-bit uniforms, rounded to float; its u1 <= 1e-300 clamp
+    // (src/astrosim_fused.cu:146) becomes log(1e-300) for an all-zero draw
+    const double d1 = rng_uniform_at(base, 0);
+    const double d2 = rng_uniform_at(base, 1);
+    const float l1 = d1 > 0.0 ? log_fast(static_cast<float>(d1)) : -690.775528f;
+    return sqrt_ftz(-2.0f * l1) * cos_ftz(static_cast<float>(kTwoPi) * static_cast<float>(d2));
+#else
     const u32 a = static_cast<u32>(rng_mix(base) >> 40);
     const u32 b = static_cast<u32>(rng_mix(base + kCounterMul) >> 40);
     const float u1 = (static_cast<float>(a) + 0.5f) * (1.0f / 16777216.0f);
     const float u2 = static_cast<float>(b) * (1.0f / 16777216.0f);
     return sqrt_ftz(-2.0f * log_fast(u1)) * cos_ftz(static_cast<float>(kTwoPi) * u2);
+#endif
 }
 
 }  // namespace astrosim

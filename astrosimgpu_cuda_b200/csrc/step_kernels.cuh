@@ -61,7 +61,7 @@ template <typename R>
 __device__ __forceinline__ void astro_stage(const AstroK& c, R Ct, R I0, R tI, R inv_tI, R Ca, R IP3, R h, R noise,
                                             R& dCa, R& dIP3, R& dh) {
     if constexpr (std::is_same<R, float>::value) {
-        astro_rhs_fast(c, Ct, I0, inv_tI, Ca, IP3, h, noise, dCa, dIP3, dh);
+        astro_rhs_fast(c, Ct, I0, tI, inv_tI, Ca, IP3, h, noise, dCa, dIP3, dh);
     } else {
         astro_rhs(c, Ct, I0, tI, inv_tI, Ca, IP3, h, noise, dCa, dIP3, dh);
     }
