@@ -16,6 +16,7 @@ ERR_NO_DEVICE = 5
 ERR_TIMEOUT = 6
 ERR_STATE = 7
 ERR_IO = 8
+ERR_PEER = 9
 
 PRECISION_FP64 = 0
 PRECISION_FP32 = 1

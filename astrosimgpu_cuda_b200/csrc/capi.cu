@@ -562,6 +562,18 @@ int astrosim_shard_last_step_ms(astrosim_shard* s, double* ms) {
     return ASTROSIM_OK;
 }
 
+int astrosim_shard_set_timeout(astrosim_shard* s, double seconds) {
+    if (!s) return fail(ASTROSIM_ERR_INVALID_ARG, "null handle");
+    if (!(seconds > 0.0) || !std::isfinite(seconds)) return fail(ASTROSIM_ERR_INVALID_ARG, "seconds must be > 0");
+    s->r.set_timeout(seconds);
+    g_last_error.clear();
+    return ASTROSIM_OK;
+}
+
+int astrosim_shard_selftest_wait(int scenario, double timeout_s, int* windows_done, int* aborted, double* waited_s) {
+    return guarded([&] { return astrosim::selftest_bounded_wait(scenario, timeout_s, windows_done, aborted, waited_s); });
+}
+
 int astrosim_shard_destroy(astrosim_shard* s) {
     delete s;
     return ASTROSIM_OK;

@@ -5,8 +5,10 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <thread>
 
 #include "shard.cuh"
 #include "window_kernels.cuh"
@@ -189,15 +191,118 @@ Status push_phase(ShardSim& s, i64 k) {
     return Status::Ok();
 }
 
+}  // namespace
+
+// ---------------------------------------------------------------- bounded waits
+double default_shard_timeout() {
+    if (const char* env = std::getenv("ASTROSIM_SHARD_TIMEOUT_S")) {
+        const double v = std::atof(env);
+        if (v > 0.0) return v;
+    }
+    return 120.0;
+}
+
+Status bounded_wait(ShardComm* comm, const std::function<int()>& query, double timeout_s, const char* what) {
+    using clock = std::chrono::steady_clock;
+    const auto start = clock::now();
+    const auto deadline = start + std::chrono::duration_cast<clock::duration>(std::chrono::duration<double>(timeout_s));
+    auto next_poll = start;
+    for (u64 it = 0;; ++it) {
+        const int q = query();
+        if (q == 0) return Status::Ok();
+        if (q < 0) {
+            if (comm) comm->abort();
+            return make_error(ASTROSIM_ERR_CUDA, "%s: the device work failed", what);
+        }
+        const auto now = clock::now();
+        if (comm && now >= next_poll) {  // the communicator's view of its peers, every 10 ms
+            bool pending = false;
+            Status st = comm->async_state(&pending);
+            if (!st.ok()) {
+                comm->abort();
+                return make_error(ASTROSIM_ERR_PEER, "%s: %s", what, st.msg.c_str());
+            }
+            next_poll = now + std::chrono::milliseconds(10);
+        }
+        if (now >= deadline) {
+            if (comm) comm->abort();
+            return make_error(ASTROSIM_ERR_TIMEOUT,
+                              "%s: no progress within %.3g s (a rank failed or left); the communicator is aborted",
+                              what, timeout_s);
+        }
+        // spin for the first ~2 ms (an exchange usually completes within that), then back off
+        if (now - start > std::chrono::milliseconds(2)) std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+}
+
+Status bounded_stream_wait(ShardComm* comm, cudaStream_t st, double timeout_s, const char* what) {
+    return bounded_wait(
+        comm,
+        [st]() {
+            const cudaError_t e = cudaStreamQuery(st);
+            if (e == cudaSuccess) return 0;
+            if (e == cudaErrorNotReady) return 1;
+            cudaGetLastError();
+            return -1;
+        },
+        timeout_s, what);
+}
+
+namespace {
+
+// A communicator whose peers behave as one failure scenario prescribes (no device).
+class StandInComm : public ShardComm {
+public:
+    explicit StandInComm(int scenario) : scenario_(scenario) {}
+    Status all_gather(const void*, void*, size_t, cudaStream_t) override { return Status::Ok(); }
+    Status async_state(bool* pending) override {
+        *pending = false;
+        if (scenario_ == 2 && ++polls_ >= 3) return make_error(ASTROSIM_ERR_PEER, "a peer reported a failure");
+        return Status::Ok();
+    }
+    void abort() override { aborted = true; }
+    bool aborted = false;
+
+private:
+    int scenario_;
+    int polls_ = 0;
+};
+
+}  // namespace
+
+Status selftest_bounded_wait(int scenario, double timeout_s, int* windows_done, int* aborted, double* waited_s) {
+    if (scenario < 0 || scenario > 3) return make_error(ASTROSIM_ERR_INVALID_ARG, "scenario must be 0-3");
+    if (!(timeout_s > 0.0)) return make_error(ASTROSIM_ERR_INVALID_ARG, "timeout_s must be > 0");
+    StandInComm comm(scenario);
+    const auto t0 = std::chrono::steady_clock::now();
+    int done = 0;
+    Status st;
+    for (int k = 0; k < 4 && st.ok(); ++k) {
+        // window k's exchange: complete after a few polls, or never (a rank that left)
+        const bool never = scenario == 1 || scenario == 2 || (scenario == 3 && k >= 2);
+        int polls = 0;
+        st = bounded_wait(&comm, [&]() { return (!never && ++polls > 3) ? 0 : 1; }, timeout_s, "window exchange");
+        if (st.ok()) ++done;
+    }
+    if (windows_done) *windows_done = done;
+    if (aborted) *aborted = comm.aborted ? 1 : 0;
+    if (waited_s) *waited_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return st;
+}
+
+namespace {
+
 // ---------------------------------------------------------------- NCCL, loaded at run time
 struct NcclApi {
     void* lib = nullptr;
     ncclResult_t (*get_unique_id)(ncclUniqueId*) = nullptr;
-    ncclResult_t (*comm_init_rank)(ncclComm_t*, int, ncclUniqueId, int) = nullptr;
+    ncclResult_t (*comm_init_rank_config)(ncclComm_t*, int, ncclUniqueId, int, ncclConfig_t*) = nullptr;
     ncclResult_t (*all_gather)(const void*, void*, size_t, ncclDataType_t, ncclComm_t, cudaStream_t) = nullptr;
     ncclResult_t (*group_start)() = nullptr;
     ncclResult_t (*group_end)() = nullptr;
     ncclResult_t (*comm_destroy)(ncclComm_t) = nullptr;
+    ncclResult_t (*comm_abort)(ncclComm_t) = nullptr;
+    ncclResult_t (*get_async_error)(ncclComm_t, ncclResult_t*) = nullptr;
     const char* (*error_string)(ncclResult_t) = nullptr;
 };
 
@@ -215,14 +320,17 @@ Status nccl_api(NcclApi** out) {
         } else {
             auto sym = [&](const char* name) { return dlsym(api.lib, name); };
             api.get_unique_id = reinterpret_cast<decltype(api.get_unique_id)>(sym("ncclGetUniqueId"));
-            api.comm_init_rank = reinterpret_cast<decltype(api.comm_init_rank)>(sym("ncclCommInitRank"));
+            api.comm_init_rank_config =
+                reinterpret_cast<decltype(api.comm_init_rank_config)>(sym("ncclCommInitRankConfig"));
             api.all_gather = reinterpret_cast<decltype(api.all_gather)>(sym("ncclAllGather"));
             api.group_start = reinterpret_cast<decltype(api.group_start)>(sym("ncclGroupStart"));
             api.group_end = reinterpret_cast<decltype(api.group_end)>(sym("ncclGroupEnd"));
             api.comm_destroy = reinterpret_cast<decltype(api.comm_destroy)>(sym("ncclCommDestroy"));
+            api.comm_abort = reinterpret_cast<decltype(api.comm_abort)>(sym("ncclCommAbort"));
+            api.get_async_error = reinterpret_cast<decltype(api.get_async_error)>(sym("ncclCommGetAsyncError"));
             api.error_string = reinterpret_cast<decltype(api.error_string)>(sym("ncclGetErrorString"));
-            if (!api.get_unique_id || !api.comm_init_rank || !api.all_gather || !api.group_start || !api.group_end ||
-                !api.comm_destroy || !api.error_string)
+            if (!api.get_unique_id || !api.comm_init_rank_config || !api.all_gather || !api.group_start ||
+                !api.group_end || !api.comm_destroy || !api.comm_abort || !api.get_async_error || !api.error_string)
                 status = make_error(ASTROSIM_ERR_UNSUPPORTED, "libnccl.so.2 lacks an entry point");
         }
     }
@@ -230,43 +338,72 @@ Status nccl_api(NcclApi** out) {
     return status;
 }
 
-#define AS_NCCL(api, call)                                                                                     \
-    do {                                                                                                      \
-        const ncclResult_t _r = (call);                                                                        \
-        if (_r != ncclSuccess) return make_error(ASTROSIM_ERR_CUDA, "%s failed: %s", #call, (api)->error_string(_r)); \
-    } while (0)
-
+// A non-blocking communicator: set-up and every enqueue may return ncclInProgress,
+// and ncclCommGetAsyncError then reports when it has finished, so each wait has a
+// deadline and a communicator whose peer vanished is aborted instead of hanging.
 class NcclComm : public ShardComm {
 public:
     ~NcclComm() override {
         if (comm_) api_->comm_destroy(comm_);
     }
-    Status init(const unsigned char id[128], int rank, int world, int device) {
+    Status init(const unsigned char id[128], int rank, int world, int device, double timeout_s) {
         AS_TRY(nccl_api(&api_));
         AS_CUDA(cudaSetDevice(device));
+        timeout_s_ = timeout_s;
         ncclUniqueId uid;
         static_assert(sizeof(uid) == 128, "ncclUniqueId is 128 bytes");
         std::memcpy(&uid, id, sizeof(uid));
-        AS_NCCL(api_, api_->comm_init_rank(&comm_, world, uid, rank));
+        ncclConfig_t config = NCCL_CONFIG_INITIALIZER;
+        config.blocking = 0;
+        AS_TRY(settle(api_->comm_init_rank_config(&comm_, world, uid, rank, &config), "ncclCommInitRankConfig"));
         return Status::Ok();
     }
     Status all_gather(const void* send, void* recv, size_t bytes, cudaStream_t st) override {
         if (bytes == 0) return Status::Ok();
-        AS_NCCL(api_, api_->all_gather(send, recv, bytes, ncclUint8, comm_, st));
+        return settle(api_->all_gather(send, recv, bytes, ncclUint8, comm_, st), "ncclAllGather");
+    }
+    Status group_begin() override { return settle(api_->group_start(), "ncclGroupStart"); }
+    Status group_end() override { return settle(api_->group_end(), "ncclGroupEnd"); }
+    Status async_state(bool* pending) override {
+        *pending = false;
+        if (!comm_) return make_error(ASTROSIM_ERR_PEER, "the communicator was aborted");
+        ncclResult_t state = ncclSuccess;
+        const ncclResult_t r = api_->get_async_error(comm_, &state);
+        if (r != ncclSuccess) return make_error(ASTROSIM_ERR_PEER, "ncclCommGetAsyncError: %s", api_->error_string(r));
+        if (state == ncclInProgress) {
+            *pending = true;
+            return Status::Ok();
+        }
+        if (state != ncclSuccess) return make_error(ASTROSIM_ERR_PEER, "NCCL: %s", api_->error_string(state));
         return Status::Ok();
     }
-    Status group_begin() override {
-        AS_NCCL(api_, api_->group_start());
-        return Status::Ok();
-    }
-    Status group_end() override {
-        AS_NCCL(api_, api_->group_end());
-        return Status::Ok();
+    void abort() override {
+        if (comm_) api_->comm_abort(comm_);
+        comm_ = nullptr;
     }
 
 private:
+    // A call's result once it has settled: ncclInProgress is polled to completion
+    // under the deadline.
+    Status settle(ncclResult_t r, const char* what) {
+        if (r == ncclSuccess) return Status::Ok();
+        if (r != ncclInProgress) {
+            abort();
+            return make_error(ASTROSIM_ERR_PEER, "%s failed: %s", what, api_->error_string(r));
+        }
+        Status st;
+        return bounded_wait(
+            this,
+            [&]() {
+                bool pending = false;
+                st = async_state(&pending);
+                return !st.ok() ? -1 : (pending ? 1 : 0);
+            },
+            timeout_s_, what);
+    }
     NcclApi* api_ = nullptr;
     ncclComm_t comm_ = nullptr;
+    double timeout_s_ = 120.0;
 };
 
 }  // namespace
@@ -275,14 +412,16 @@ Status nccl_unique_id(unsigned char id[128]) {
     NcclApi* api = nullptr;
     AS_TRY(nccl_api(&api));
     ncclUniqueId uid;
-    AS_NCCL(api, api->get_unique_id(&uid));
+    const ncclResult_t r = api->get_unique_id(&uid);
+    if (r != ncclSuccess) return make_error(ASTROSIM_ERR_CUDA, "ncclGetUniqueId failed: %s", api->error_string(r));
     std::memcpy(id, &uid, 128);
     return Status::Ok();
 }
 
-Status make_nccl_comm(const unsigned char id[128], int rank, int world, int device, std::unique_ptr<ShardComm>& out) {
+Status make_nccl_comm(const unsigned char id[128], int rank, int world, int device, double timeout_s,
+                      std::unique_ptr<ShardComm>& out) {
     auto c = std::make_unique<NcclComm>();
-    AS_TRY(c->init(id, rank, world, device));
+    AS_TRY(c->init(id, rank, world, device, timeout_s));
     out = std::move(c);
     return Status::Ok();
 }
@@ -386,12 +525,29 @@ Status ShardRank::create(const astrosim_config& cfg, const char* biology_json, i
 Status ShardRank::connect(const unsigned char id[128]) {
     if (!s_) return make_error(ASTROSIM_ERR_STATE, "create the shard first");
     if (s_->world == 1) return Status::Ok();
-    return make_nccl_comm(id, s_->rank, s_->world, s_->device(), comm_);
+    Status st = make_nccl_comm(id, s_->rank, s_->world, s_->device(), timeout_s_, comm_);
+    if (!st.ok()) failed_ = true;
+    return st;
+}
+
+Status ShardRank::usable() const {
+    if (!s_) return make_error(ASTROSIM_ERR_STATE, "create the shard first");
+    if (failed_)
+        return make_error(ASTROSIM_ERR_STATE,
+                          "an earlier wait on the other ranks failed; the communicator is aborted and the "
+                          "network is mid-window: destroy this rank");
+    if (!comm_ && s_->world > 1) return make_error(ASTROSIM_ERR_STATE, "connect the ranks first");
+    return Status::Ok();
+}
+
+Status ShardRank::wait(const char* what) {
+    Status st = bounded_stream_wait(comm_.get(), s_->stream(), timeout_s_, what);
+    if (!st.ok()) failed_ = true;
+    return st;
 }
 
 Status ShardRank::step(i64 n) {
-    if (!s_) return make_error(ASTROSIM_ERR_STATE, "create the shard first");
-    if (!comm_ && s_->world > 1) return make_error(ASTROSIM_ERR_STATE, "connect the ranks first");
+    AS_TRY(usable());
     ShardSim& s = *s_;
     const int W = s.window();
     AS_TRY(check_whole_windows(s.sim, W, n));
@@ -410,9 +566,12 @@ Status ShardRank::step(i64 n) {
             if (s.world == 1) return s.push(k);  // nothing to exchange
             AS_TRY(s.pack(k));
             AS_TRY(comm_->all_gather(s.x_cnt.get(), s.r_cnt.get(), 2 * sizeof(u32), st));
-            std::vector<u32> c(2 * s.world);
-            AS_CUDA(cudaMemcpyAsync(c.data(), s.r_cnt.get(), c.size() * sizeof(u32), cudaMemcpyDeviceToHost, st));
-            AS_CUDA(cudaStreamSynchronize(st));
+            // pinned destination: a copy into pageable memory would block until the
+            // all-gather ends, outside the deadline
+            u32* hc = s.host_counts_buffer();
+            AS_CUDA(cudaMemcpyAsync(hc, s.r_cnt.get(), 2 * s.world * sizeof(u32), cudaMemcpyDeviceToHost, st));
+            AS_TRY(wait("window count exchange"));
+            const std::vector<u32> c(hc, hc + 2 * s.world);
             u64 ms = 0, ma = 0;
             for (int r = 0; r < s.world; ++r) {
                 ms = std::max<u64>(ms, c[2 * r]);
@@ -430,8 +589,14 @@ Status ShardRank::step(i64 n) {
         }();
         s.note_window(std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
     }
+    if (!status.ok()) failed_ = true;  // a window stopped part-way
     AS_CUDA(cudaEventRecord(e1, st));
-    AS_CUDA(cudaEventSynchronize(e1));
+    if (status.ok()) status = wait("window exchange");
+    if (!status.ok()) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        return status;
+    }
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);
     last_ms_ = ms;
@@ -442,7 +607,7 @@ Status ShardRank::step(i64 n) {
 
 Status ShardRank::gather(int which) {
     if (s_->world == 1) return Status::Ok();
-    if (!comm_) return make_error(ASTROSIM_ERR_STATE, "connect the ranks first");
+    AS_TRY(usable());
     ShardSim& s = *s_;
     void* base = nullptr;
     size_t elem = 0;
@@ -476,12 +641,11 @@ Status ShardRank::gather(int which) {
             AS_CUDA(cudaMemcpyAsync(b + lo * elem, recv.get() + r * max_len * elem, len * elem,
                                     cudaMemcpyDeviceToDevice, st));
     }
-    AS_CUDA(cudaStreamSynchronize(st));
-    return Status::Ok();
+    return wait("state gather");
 }
 
 Status ShardRank::summary(astrosim_summary_t& out) {
-    if (!s_) return make_error(ASTROSIM_ERR_STATE, "create the shard first");
+    AS_TRY(usable());
     AS_TRY(gather(ASTROSIM_STATE_CA));
     // the engaged flags sit beside the state arrays; gather them as bytes
     if (s_->world > 1) {
@@ -506,13 +670,13 @@ Status ShardRank::summary(astrosim_summary_t& out) {
             if (r != s.rank && l)
                 AS_CUDA(cudaMemcpyAsync(ev + plans[r].a_lo, recv.get() + r * max_len, l, cudaMemcpyDeviceToDevice, st));
         }
-        AS_CUDA(cudaStreamSynchronize(st));
+        AS_TRY(wait("engaged-flag gather"));
     }
     return s_->sim.summary(out);
 }
 
 Status ShardRank::get_state(int which, double* dst, size_t count) {
-    if (!s_) return make_error(ASTROSIM_ERR_STATE, "create the shard first");
+    AS_TRY(usable());
     AS_TRY(gather(which));
     return s_->sim.get_state(which, dst, count);
 }

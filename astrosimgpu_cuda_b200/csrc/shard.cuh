@@ -15,6 +15,7 @@
 // results are bit-identical to the single-GPU run.
 #pragma once
 
+#include <functional>
 #include <memory>
 #include <vector>
 
@@ -40,11 +41,43 @@ public:
     virtual Status all_gather(const void* send, void* recv, size_t bytes, cudaStream_t st) = 0;
     virtual Status group_begin() { return Status::Ok(); }
     virtual Status group_end() { return Status::Ok(); }
+    // The communicator's own view of its peers: an ASTROSIM_ERR_PEER status once it
+    // has seen a peer fail or leave; *pending while it is still setting up.
+    virtual Status async_state(bool* pending) {
+        *pending = false;
+        return Status::Ok();
+    }
+    // Ends every operation of this communicator still in flight (the communicator
+    // is unusable afterwards): the way out of a wait on a peer that never comes.
+    virtual void abort() {}
 };
 
-// NCCL communicator (libnccl.so.2 loaded at run time) for one rank per process.
+// Polls `query` (0: the work is done, 1: still running, -1: it failed) until it
+// reports done, the communicator reports a failed peer, or `timeout_s` passes.  On
+// a failed peer or an expired deadline it aborts the communicator and returns
+// ASTROSIM_ERR_PEER or ASTROSIM_ERR_TIMEOUT, so no rank waits for ever on a rank
+// that died or left; `what` names the wait in the message.
+Status bounded_wait(ShardComm* comm, const std::function<int()>& query, double timeout_s, const char* what);
+
+// bounded_wait on everything enqueued on stream `st` so far.
+Status bounded_stream_wait(ShardComm* comm, cudaStream_t st, double timeout_s, const char* what);
+
+// Exercises bounded_wait with a stand-in communicator and stand-in exchanges (no
+// device, no NCCL): scenario 0, four windows whose exchanges complete; 1, the first
+// exchange never completes; 2, the communicator reports a failed peer during the
+// first exchange; 3, the exchanges of windows 0 and 1 complete, then a rank has
+// left and the exchange of window 2 never completes.
+Status selftest_bounded_wait(int scenario, double timeout_s, int* windows_done, int* aborted, double* waited_s);
+
+// Seconds a rank waits on the others before it gives up: ASTROSIM_SHARD_TIMEOUT_S,
+// else 120.
+double default_shard_timeout();
+
+// NCCL communicator (libnccl.so.2 loaded at run time) for one rank per process;
+// non-blocking, so that set-up and every exchange can be given a deadline.
 Status nccl_unique_id(unsigned char id[128]);
-Status make_nccl_comm(const unsigned char id[128], int rank, int world, int device, std::unique_ptr<ShardComm>& out);
+Status make_nccl_comm(const unsigned char id[128], int rank, int world, int device, double timeout_s,
+                      std::unique_ptr<ShardComm>& out);
 
 // One rank's part of a sharded network.
 class ShardSim {
@@ -60,6 +93,7 @@ public:
     void note_window(double seconds);
 
     const u32* host_counts() const { return h_cnt_; }
+    u32* host_counts_buffer() { return h_cnt_; }  // pinned, 2 * world entries
     cudaStream_t stream() const { return sim.stream(); }
     int device() const { return sim.config().device; }
     size_t real_bytes() const { return sim.fp32() ? sizeof(float) : sizeof(double); }
@@ -92,12 +126,19 @@ public:
     ShardSim& shard() { return *s_; }
     bool has_shard() const { return static_cast<bool>(s_); }
     double last_step_ms() const { return last_ms_; }
+    // Deadline of every wait on the other ranks (set-up included), seconds.
+    void set_timeout(double seconds) { timeout_s_ = seconds; }
+    double timeout() const { return timeout_s_; }
 
 private:
     Status gather(int which);
+    Status wait(const char* what);  // bounded wait on this rank's stream
+    Status usable() const;
     std::unique_ptr<ShardSim> s_;
     std::unique_ptr<ShardComm> comm_;
     double last_ms_ = 0.0;
+    double timeout_s_ = default_shard_timeout();
+    bool failed_ = false;  // a wait gave up: the communicator is aborted, the state is mid-window
 };
 
 // All ranks of a sharded network in one process: devices[r] runs rank r (devices

@@ -32,6 +32,9 @@ def _lib():
         L.astrosim_shard_spike_counts.argtypes = [P, C.c_int64, C.c_int64, u32p]
         L.astrosim_shard_last_step_ms.argtypes = [P, C.POINTER(C.c_double)]
         L.astrosim_shard_destroy.argtypes = [P]
+        L.astrosim_shard_set_timeout.argtypes = [P, C.c_double]
+        L.astrosim_shard_selftest_wait.argtypes = [C.c_int, C.c_double, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                                   C.POINTER(C.c_double)]
         L.astrosim_shard_group_create.argtypes = [C.POINTER(abi.Config), C.c_char_p, C.c_int,
                                                   C.POINTER(C.c_int), C.POINTER(P)]
         L.astrosim_shard_group_step.argtypes = [P, C.c_int64]
@@ -55,6 +58,16 @@ def shard_plan(n_total, rank, world):
     v = [C.c_uint32() for _ in range(4)]
     check(_lib().astrosim_shard_plan(n_total, rank, world, *[C.byref(x) for x in v]))
     return tuple(x.value for x in v)
+
+
+def selftest_wait(scenario, timeout_s):
+    """The deadline logic of the ranks' waits on a stand-in communicator (no device):
+    (status, windows completed, stand-in aborted, seconds).  Scenarios as
+    astrosim_shard_selftest_wait in include/astrosim.h."""
+    done, aborted, waited = C.c_int(), C.c_int(), C.c_double()
+    rc = _lib().astrosim_shard_selftest_wait(int(scenario), float(timeout_s), C.byref(done), C.byref(aborted),
+                                             C.byref(waited))
+    return rc, done.value, bool(aborted.value), waited.value
 
 
 def unique_id():
@@ -157,7 +170,9 @@ def share_id(make_id=unique_id, group=None):
 class ShardedSimulation:
     """This process's rank of one network split across the torch.distributed group."""
 
-    def __init__(self, cfg=None, biology=None, group=None, **overrides):
+    def __init__(self, cfg=None, biology=None, group=None, timeout_s=None, **overrides):
+        """`timeout_s`: deadline of every wait on the other ranks (astrosim_shard_set_timeout);
+        a rank that died or left then makes the others raise instead of hanging."""
         import torch.distributed as dist
         self.cfg = cfg if cfg is not None else default_config(**overrides)
         if dist.is_available() and dist.is_initialized():
@@ -176,6 +191,8 @@ class ShardedSimulation:
             all_ranks_ok(rc == abi.OK, msg, group)  # nobody joins the communicator if a rank failed
         else:
             check(rc)
+        if timeout_s is not None:
+            check(_lib().astrosim_shard_set_timeout(self._h, float(timeout_s)))
         ident = share_id(group=group) if self.world > 1 else b"\0" * 128
         check(_lib().astrosim_shard_connect(self._h, ident))
         self.plan = shard_plan(self.cfg.n_total, self.rank, self.world)

@@ -33,9 +33,11 @@ enum {
     ASTROSIM_ERR_OUT_OF_MEMORY = 3, /* device allocation failed */
     ASTROSIM_ERR_UNSUPPORTED = 4,   /* configuration outside what the kernels implement */
     ASTROSIM_ERR_NO_DEVICE = 5,     /* no CUDA device visible (reference: src/astrosim_fused.cu:906-912) */
-    ASTROSIM_ERR_TIMEOUT = 6,       /* a bounded device-side wait gave up */
+    ASTROSIM_ERR_TIMEOUT = 6,       /* a bounded wait gave up: device-side, or on the other ranks of a
+                                       sharded network (a rank that died or left) */
     ASTROSIM_ERR_STATE = 7,         /* call not valid in the handle's current state */
-    ASTROSIM_ERR_IO = 8             /* a host file could not be written */
+    ASTROSIM_ERR_IO = 8,            /* a host file could not be written */
+    ASTROSIM_ERR_PEER = 9           /* another rank of a sharded network failed (reported by the communicator) */
 };
 
 enum {
@@ -424,7 +426,25 @@ int astrosim_shard_get_state(astrosim_shard* s, int which, double* dst, size_t c
 int astrosim_shard_spike_counts(astrosim_shard* s, int64_t first_step, int64_t n, uint32_t* counts);
 /* Device time of this rank's last astrosim_shard_step, ms (take the max over ranks). */
 int astrosim_shard_last_step_ms(astrosim_shard* s, double* ms);
+/* Deadline, in seconds, of every wait on the other ranks (connect, each window's
+   exchange, the gathers of summary and get_state); default ASTROSIM_SHARD_TIMEOUT_S
+   from the environment, else 120.  The communicator is non-blocking: when a wait
+   passes its deadline (a rank died or left between windows) the call aborts the
+   communicator and returns ASTROSIM_ERR_TIMEOUT, and when the communicator reports
+   a failed peer it returns ASTROSIM_ERR_PEER.  Either way this rank stays unusable
+   (ASTROSIM_ERR_STATE) until destroyed.  The reference has no counterpart: it runs
+   on one GPU and aborts the process on any CUDA error (src/astrosim_fused.cu:109-117). */
+int astrosim_shard_set_timeout(astrosim_shard* s, double seconds);
 int astrosim_shard_destroy(astrosim_shard* s);
+
+/* The deadline logic of the waits above, run on a stand-in communicator with no
+   device and no NCCL.  Scenario 0: four windows whose exchanges complete;
+   1: the first window's exchange never completes; 2: the communicator reports a
+   failed peer during the first exchange; 3: windows 0 and 1 complete, then a rank
+   has left and window 2's exchange never completes.  Returns the status the wait
+   returned and reports the windows that completed, whether the stand-in was
+   aborted, and the seconds spent.  No counterpart in the reference. */
+int astrosim_shard_selftest_wait(int scenario, double timeout_s, int* windows_done, int* aborted, double* waited_s);
 
 /* All ranks in this process: rank r runs on devices[r] (NULL: every rank on
    cfg.device; ranks that share a device run one after another).  Same results. */
