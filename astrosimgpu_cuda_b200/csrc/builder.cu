@@ -186,12 +186,40 @@ Status edges_to_csr(const u32* src, const u32* dst, u64 n, u32 n_targets, Device
     return Status::Ok();
 }
 
-Status edge_lists_to_network(const EdgeLists& e, const u64 counts[3], const Sizes& sz, Network& net,
-                             cudaStream_t st) {
-    AS_TRY(edges_to_csr(e.exc_src, e.exc_dst, counts[0], sz.n_neurons, net.exc, st));
-    AS_TRY(edges_to_csr(e.inh_src, e.inh_dst, counts[1], sz.n_neurons, net.inh, st));
-    AS_TRY(edges_to_csr(e.sic_src, e.sic_dst, counts[2], sz.n_neurons, net.sic, st));
-    AS_TRY(edges_to_csr(e.e2a_src, e.e2a_dst, counts[2], sz.n_astro, net.e2a, st));
+Status edge_lists_to_network(const EdgeLists& e, const u64 counts[4], Network& net, cudaStream_t st) {
+    const u32 nn = net.own.n_hi - net.own.n_lo, na = net.own.a_hi - net.own.a_lo;
+    AS_TRY(edges_to_csr(e.exc_src, e.exc_dst, counts[0], nn, net.exc, st));
+    AS_TRY(edges_to_csr(e.inh_src, e.inh_dst, counts[1], nn, net.inh, st));
+    AS_TRY(edges_to_csr(e.e2a_src, e.e2a_dst, counts[2], na, net.e2a, st));
+    AS_TRY(edges_to_csr(e.sic_src, e.sic_dst, counts[3], nn, net.sic, st));
+    return Status::Ok();
+}
+
+__global__ void slice_rows_kernel(const u32* rs, u32 lo, u32 n_rows, u32* out) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i <= n_rows) out[i] = rs[lo + i] - rs[lo];
+}
+
+Status slice_csr(DeviceCSR& c, u32 lo, u32 hi, cudaStream_t st) {
+    if (lo == 0 && hi == c.n_targets) return Status::Ok();
+    std::vector<u32> ends(2);
+    AS_CUDA(cudaMemcpyAsync(&ends[0], c.row_start.get() + lo, sizeof(u32), cudaMemcpyDeviceToHost, st));
+    AS_CUDA(cudaMemcpyAsync(&ends[1], c.row_start.get() + hi, sizeof(u32), cudaMemcpyDeviceToHost, st));
+    AS_CUDA(cudaStreamSynchronize(st));
+    DeviceCSR out;
+    out.n_targets = hi - lo;
+    out.n_edges = ends[1] - ends[0];
+    AS_TRY(out.row_start.alloc(static_cast<size_t>(out.n_targets) + 1));
+    AS_TRY(out.src.alloc(out.n_edges));
+    slice_rows_kernel<<<ceil_div(static_cast<u64>(out.n_targets) + 1, 256), 256, 0, st>>>(c.row_start.get(), lo,
+                                                                                        out.n_targets,
+                                                                                        out.row_start.get());
+    AS_CUDA(cudaGetLastError());
+    if (out.n_edges)
+        AS_CUDA(cudaMemcpyAsync(out.src.get(), c.src.get() + ends[0], out.n_edges * sizeof(u32),
+                                cudaMemcpyDeviceToDevice, st));
+    AS_CUDA(cudaStreamSynchronize(st));
+    c = std::move(out);
     return Status::Ok();
 }
 
@@ -332,8 +360,8 @@ Status build_sequential(const Sizes& sz, u64 seed, u64 c0, Network& net, cudaStr
         unsigned long long counts[4];
         AS_CUDA(cudaMemcpyAsync(counts, s.counts.get(), sizeof(counts), cudaMemcpyDeviceToHost, st));
         AS_CUDA(cudaStreamSynchronize(st));
-        const u64 c3[3] = {counts[0], counts[1], counts[2]};
-        return edge_lists_to_network(s.view(), c3, sz, net, st);
+        const u64 c3[4] = {counts[0], counts[1], counts[2], counts[2]};
+        return edge_lists_to_network(s.view(), c3, net, st);
     }
     return make_error(ASTROSIM_ERR_CUDA, "skip tie-break table did not settle");
 }
@@ -371,10 +399,24 @@ Status build_network(const Sizes& sz, u64 seed, const Biology& bio, const BuildO
         if (std::strcmp(env, "sequential") == 0) threshold = ~0ull;
         else if (std::strcmp(env, "parallel") == 0) threshold = 0;
     }
+    net.own = opt.own.clamped(sz);
     if (est <= static_cast<double>(threshold)) {
+        // a small network: the one-thread walk builds every row, then the owned rows are kept
         net.builder_path = 0;
+        const CellRange own = net.own;
+        net.own = CellRange{}.clamped(sz);
         AS_TRY(build_sequential(sz, seed, c0, net, st));
+        net.total_edges[0] = net.exc.n_edges;
+        net.total_edges[1] = net.inh.n_edges;
+        net.total_edges[2] = net.e2a.n_edges;
+        net.total_edges[3] = net.sic.n_edges;
+        net.own = own;
+        AS_TRY(slice_csr(net.exc, own.n_lo, own.n_hi, st));
+        AS_TRY(slice_csr(net.inh, own.n_lo, own.n_hi, st));
+        AS_TRY(slice_csr(net.sic, own.n_lo, own.n_hi, st));
+        AS_TRY(slice_csr(net.e2a, own.a_lo, own.a_hi, st));
     } else {
+        // the chunked walk emits only the owned rows' edges (and counts every edge)
         net.builder_path = 1;
         AS_TRY(build_parallel(sz, seed, c0, net, st));
     }

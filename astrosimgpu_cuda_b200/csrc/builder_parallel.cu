@@ -386,11 +386,29 @@ __global__ void copy_orbit_kernel(const u64* src, u64* dst, u64 n) {
 }
 
 // ---------------------------------------------------------------- count and emit
+// Owned targets of the build (CellRange): an exc/inh edge and an a2n (sic) edge are
+// kept when their neuron target is owned, an e2a edge when its astrocyte is.
+struct Owned {
+    u32 n_lo, n_hi, a_lo, a_hi;
+    __device__ __forceinline__ bool neuron(u32 post) const { return post >= n_lo && post < n_hi; }
+    __device__ __forceinline__ bool astro(u32 a) const { return a >= a_lo && a < a_hi; }
+};
+
+// Per pre: kept primary edges, kept e2a edges, kept sic edges; and every edge for
+// the whole network's totals.
 struct CountVisit {
-    u64 ne = 0, nt = 0;
-    __device__ __forceinline__ void operator()(u32, bool hit, u32) {
-        ++ne;
-        nt += hit ? 1u : 0u;
+    Owned own;
+    u64 ne = 0, na = 0, ns = 0;
+    u32 te = 0, tt = 0;
+    __device__ __forceinline__ void operator()(u32 post, bool hit, u32 astro) {
+        const bool pn = own.neuron(post);
+        ++te;
+        ne += pn ? 1u : 0u;
+        if (hit) {
+            ++tt;
+            na += own.astro(astro) ? 1u : 0u;
+            ns += pn ? 1u : 0u;
+        }
     }
 };
 
@@ -398,39 +416,62 @@ __device__ __forceinline__ u32 self_post_of(int mode, u32 r, u32 self_off) {
     return mode == 0 ? kNoSelf : r + self_off;  // mode 1: autapse at post == r + self_off
 }
 
-__global__ void count_kernel(Sec s, const u64* orbit, u64 n, int self_mode, u32 self_off, u64* ce, u64* ct) {
+// totals[0] += every primary edge, totals[1] += every third-factor edge (one atomic per warp).
+__global__ void count_kernel(Sec s, const u64* orbit, u64 n, int self_mode, u32 self_off, Owned own, u64* ce,
+                             u64* ca, u64* cs, unsigned long long* totals) {
     const u64 r = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (r >= n) return;
-    CountVisit v;
-    walk_pre(s, orbit[r], self_post_of(self_mode, static_cast<u32>(r), self_off), v);
-    ce[r] = v.ne;
-    ct[r] = v.nt;
+    CountVisit v{own};
+    if (r < n) {
+        walk_pre(s, orbit[r], self_post_of(self_mode, static_cast<u32>(r), self_off), v);
+        ce[r] = v.ne;
+        ca[r] = v.na;
+        cs[r] = v.ns;
+    }
+    unsigned long long te = v.te, tt = v.tt;
+    for (int off = 16; off > 0; off >>= 1) {
+        te += __shfl_down_sync(0xffffffffu, te, off);
+        tt += __shfl_down_sync(0xffffffffu, tt, off);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&totals[0], te);
+        atomicAdd(&totals[1], tt);
+    }
 }
 
 struct EmitVisit {
+    Owned own;
     u32 pre;
     u32 *e_src, *e_dst, *t_src, *t_dst, *s_src, *s_dst;
-    u64 oe, ot;
+    u64 oe, oa, os;
     __device__ __forceinline__ void operator()(u32 post, bool hit, u32 astro) {
-        e_src[oe] = pre;
-        e_dst[oe] = post;
-        ++oe;
+        const bool pn = own.neuron(post);
+        if (pn) {
+            e_src[oe] = pre;
+            e_dst[oe] = post - own.n_lo;
+            ++oe;
+        }
         if (hit) {
-            t_src[ot] = pre;
-            t_dst[ot] = astro;
-            s_src[ot] = astro;
-            s_dst[ot] = post;
-            ++ot;
+            if (own.astro(astro)) {
+                t_src[oa] = pre;
+                t_dst[oa] = astro - own.a_lo;
+                ++oa;
+            }
+            if (pn) {
+                s_src[os] = astro;
+                s_dst[os] = post - own.n_lo;
+                ++os;
+            }
         }
     }
 };
 
-__global__ void emit_kernel(Sec s, const u64* orbit, u64 n, int self_mode, u32 self_off, const u64* oe,
-                            const u64* ot, u64 base_e, u64 base_t, u32* e_src, u32* e_dst, u32* t_src, u32* t_dst,
-                            u32* s_src, u32* s_dst) {
+__global__ void emit_kernel(Sec s, const u64* orbit, u64 n, int self_mode, u32 self_off, Owned own, const u64* oe,
+                            const u64* oa, const u64* os, u64 base_e, u64 base_a, u64 base_s, u32* e_src,
+                            u32* e_dst, u32* t_src, u32* t_dst, u32* s_src, u32* s_dst) {
     const u64 r = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (r >= n) return;
-    EmitVisit v{static_cast<u32>(r), e_src, e_dst, t_src, t_dst, s_src, s_dst, base_e + oe[r], base_t + ot[r]};
+    EmitVisit v{own, static_cast<u32>(r), e_src, e_dst, t_src, t_dst, s_src, s_dst,
+                base_e + oe[r], base_a + oa[r], base_s + os[r]};
     walk_pre(s, orbit[r], self_post_of(self_mode, static_cast<u32>(r), self_off), v);
 }
 
@@ -777,58 +818,75 @@ Status build_parallel(const Sizes& sz, u64 seed, u64 c0, Network& net, cudaStrea
         pc.mark(plans[k].name);
     }
 
-    // ---- 5. count, scan, emit
-    DevBuf<u64> ce[3], ct[3], oe[3], ot[3];
-    u64 tot_e[3] = {0, 0, 0}, tot_t[3] = {0, 0, 0};
+    // ---- 5. count, scan, emit (only the edges whose target this network owns)
+    const Owned own{net.own.n_lo, net.own.n_hi, net.own.a_lo, net.own.a_hi};
+    DevBuf<u64> oe[3], oa[3], os[3];
+    DevBuf<unsigned long long> totals;
+    AS_TRY(totals.alloc_zero(6, st));
+    u64 tot_e[3] = {0, 0, 0}, tot_a[3] = {0, 0, 0}, tot_s[3] = {0, 0, 0};
     for (int k = 0; k < 3; ++k) {
         const SectionPlan& P = plans[k];
         s.post_count = P.post_count;
         s.post_off = P.post_off;
         s.third = P.third;
-        AS_TRY(ce[k].alloc(P.n_pres));
-        AS_TRY(ct[k].alloc(P.n_pres));
+        DevBuf<u64> ce, ca, cs;
+        AS_TRY(ce.alloc(P.n_pres));
+        AS_TRY(ca.alloc(P.n_pres));
+        AS_TRY(cs.alloc(P.n_pres));
         AS_TRY(oe[k].alloc(P.n_pres));
-        AS_TRY(ot[k].alloc(P.n_pres));
+        AS_TRY(oa[k].alloc(P.n_pres));
+        AS_TRY(os[k].alloc(P.n_pres));
         count_kernel<<<ceil_div(P.n_pres, 128), 128, 0, st>>>(s, orbits[k].get(), P.n_pres, P.self_mode, P.self_off,
-                                                             ce[k].get(), ct[k].get());
+                                                             own, ce.get(), ca.get(), cs.get(),
+                                                             totals.get() + 2 * k);
         AS_CUDA(cudaGetLastError());
-        AS_TRY(exclusive_scan_u64(ce[k].get(), oe[k].get(), P.n_pres, st));
-        AS_TRY(exclusive_scan_u64(ct[k].get(), ot[k].get(), P.n_pres, st));
-        u64 a = 0, b = 0, c = 0, d = 0;
-        AS_TRY(to_host(&a, oe[k].get() + (P.n_pres - 1), 1, st));
-        AS_TRY(to_host(&b, ce[k].get() + (P.n_pres - 1), 1, st));
-        AS_TRY(to_host(&c, ot[k].get() + (P.n_pres - 1), 1, st));
-        AS_TRY(to_host(&d, ct[k].get() + (P.n_pres - 1), 1, st));
-        tot_e[k] = a + b;
-        tot_t[k] = c + d;
-        ce[k].release();
-        ct[k].release();
+        AS_TRY(exclusive_scan_u64(ce.get(), oe[k].get(), P.n_pres, st));
+        AS_TRY(exclusive_scan_u64(ca.get(), oa[k].get(), P.n_pres, st));
+        AS_TRY(exclusive_scan_u64(cs.get(), os[k].get(), P.n_pres, st));
+        u64 h[6] = {0, 0, 0, 0, 0, 0};
+        AS_TRY(to_host(&h[0], oe[k].get() + (P.n_pres - 1), 1, st));
+        AS_TRY(to_host(&h[1], ce.get() + (P.n_pres - 1), 1, st));
+        AS_TRY(to_host(&h[2], oa[k].get() + (P.n_pres - 1), 1, st));
+        AS_TRY(to_host(&h[3], ca.get() + (P.n_pres - 1), 1, st));
+        AS_TRY(to_host(&h[4], os[k].get() + (P.n_pres - 1), 1, st));
+        AS_TRY(to_host(&h[5], cs.get() + (P.n_pres - 1), 1, st));
+        tot_e[k] = h[0] + h[1];
+        tot_a[k] = h[2] + h[3];
+        tot_s[k] = h[4] + h[5];
+    }
+    {
+        unsigned long long t[6];
+        AS_TRY(to_host(t, totals.get(), 6, st));
+        net.total_edges[0] = t[0] + t[2];  // excitatory primary edges: sections 0 and 1
+        net.total_edges[1] = t[4];         // inhibitory: section 2
+        net.total_edges[2] = t[1] + t[3];  // third-factor pairs: one e2a and one sic edge each
+        net.total_edges[3] = t[1] + t[3];
     }
     EdgeStorage es;
     es.cap_exc = tot_e[0] + tot_e[1];
     es.cap_inh = tot_e[2];
-    es.cap_third = tot_t[0] + tot_t[1];
+    const u64 cap_e2a = tot_a[0] + tot_a[1], cap_sic = tot_s[0] + tot_s[1];
     AS_TRY(es.exc_src.alloc(es.cap_exc));
     AS_TRY(es.exc_dst.alloc(es.cap_exc));
     AS_TRY(es.inh_src.alloc(es.cap_inh));
     AS_TRY(es.inh_dst.alloc(es.cap_inh));
-    AS_TRY(es.e2a_src.alloc(es.cap_third));
-    AS_TRY(es.e2a_dst.alloc(es.cap_third));
-    AS_TRY(es.sic_src.alloc(es.cap_third));
-    AS_TRY(es.sic_dst.alloc(es.cap_third));
+    AS_TRY(es.e2a_src.alloc(cap_e2a));
+    AS_TRY(es.e2a_dst.alloc(cap_e2a));
+    AS_TRY(es.sic_src.alloc(cap_sic));
+    AS_TRY(es.sic_dst.alloc(cap_sic));
     AS_TRY(es.counts.alloc_zero(4, st));
     for (int k = 0; k < 3; ++k) {
         const SectionPlan& P = plans[k];
         s.post_count = P.post_count;
         s.post_off = P.post_off;
         s.third = P.third;
-        const u64 base_e = k == 1 ? tot_e[0] : 0, base_t = k == 1 ? tot_t[0] : 0;
+        const u64 base_e = k == 1 ? tot_e[0] : 0, base_a = k == 1 ? tot_a[0] : 0, base_s = k == 1 ? tot_s[0] : 0;
         u32* e_src = k == 2 ? es.inh_src.get() : es.exc_src.get();
         u32* e_dst = k == 2 ? es.inh_dst.get() : es.exc_dst.get();
         emit_kernel<<<ceil_div(P.n_pres, 128), 128, 0, st>>>(s, orbits[k].get(), P.n_pres, P.self_mode, P.self_off,
-                                                            oe[k].get(), ot[k].get(), base_e, base_t, e_src, e_dst,
-                                                            es.e2a_src.get(), es.e2a_dst.get(), es.sic_src.get(),
-                                                            es.sic_dst.get());
+                                                            own, oe[k].get(), oa[k].get(), os[k].get(), base_e,
+                                                            base_a, base_s, e_src, e_dst, es.e2a_src.get(),
+                                                            es.e2a_dst.get(), es.sic_src.get(), es.sic_dst.get());
         AS_CUDA(cudaGetLastError());
     }
     int herr = 0;
@@ -837,13 +895,14 @@ Status build_parallel(const Sizes& sz, u64 seed, u64 c0, Network& net, cudaStrea
     for (int k = 0; k < 3; ++k) {
         orbits[k].release();
         oe[k].release();
-        ot[k].release();
+        oa[k].release();
+        os[k].release();
     }
     cache.release();
     pool.release();
     pc.mark("count + emit");
-    const u64 counts[3] = {es.cap_exc, es.cap_inh, es.cap_third};
-    AS_TRY(edge_lists_to_network(es.view(), counts, sz, net, st));
+    const u64 counts[4] = {es.cap_exc, es.cap_inh, cap_e2a, cap_sic};
+    AS_TRY(edge_lists_to_network(es.view(), counts, net, st));
     pc.mark("CSR sort");
 
     // The astrocyte out-degree cap (src/astrosim_fused.cu:702) drops a third-factor
@@ -851,7 +910,9 @@ Status build_parallel(const Sizes& sz, u64 seed, u64 c0, Network& net, cudaStrea
     // per astrocyte it never fires and the lists above are exact.
     DevBuf<unsigned> mx;
     AS_TRY(mx.alloc_zero(1, st));
-    max_row_kernel<<<ceil_div(nA, 256), 256, 0, st>>>(net.e2a.row_start.get(), nA, mx.get());
+    const u32 own_astro = net.own.a_hi - net.own.a_lo;  // each rank checks its own astrocytes
+    if (own_astro)
+        max_row_kernel<<<ceil_div(own_astro, 256), 256, 0, st>>>(net.e2a.row_start.get(), own_astro, mx.get());
     AS_CUDA(cudaGetLastError());
     unsigned hmx = 0;
     AS_TRY(to_host(&hmx, mx.get(), 1, st));

@@ -622,6 +622,22 @@ int astrosim_shard_group_spike_counts(astrosim_shard_group* g, int64_t first_ste
     return guarded([&] { return g->g.spike_counts(first_step, n, counts); });
 }
 
+int astrosim_shard_group_get_csr(astrosim_shard_group* g, int rank, int which, uint32_t* row_start, size_t row_cap,
+                                 uint32_t* src, size_t src_cap, uint32_t* first_row, uint32_t* n_rows,
+                                 uint64_t* n_edges) {
+    if (!g) return fail(ASTROSIM_ERR_INVALID_ARG, "null handle");
+    if (rank < 0 || rank >= g->g.world()) return fail(ASTROSIM_ERR_INVALID_ARG, "rank out of range");
+    return guarded([&] {
+        astrosim::Simulation& sim = g->g.shard(rank).sim;
+        const astrosim::CellRange& own = sim.network().own;
+        if (first_row) *first_row = which == ASTROSIM_CSR_E2A ? own.a_lo : own.n_lo;
+        astrosim::u64 ne = 0;
+        astrosim::Status s = sim.get_csr(which, row_start, row_cap, src, src_cap, n_rows, &ne);
+        if (n_edges) *n_edges = ne;
+        return s;
+    });
+}
+
 int astrosim_shard_group_destroy(astrosim_shard_group* g) {
     delete g;
     return ASTROSIM_OK;

@@ -19,13 +19,40 @@ struct DeviceCSR {
     u64 n_edges = 0;
 };
 
+// The cells whose incoming connections a network keeps: neurons [n_lo, n_hi) and
+// astrocytes [a_lo, a_hi).  A whole network owns every cell.  A rank of a sharded
+// network owns its range: its exc, inh and sic CSRs hold only the rows of neurons
+// [n_lo, n_hi) and its e2a CSR only those of astrocytes [a_lo, a_hi), row r being
+// cell lo + r, so each rank keeps about 1 / world of the connectivity.  The rows it
+// keeps are exactly the whole network's rows (same sources in the same order).
+struct CellRange {
+    u32 n_lo = 0, n_hi = 0xFFFFFFFFu;
+    u32 a_lo = 0, a_hi = 0xFFFFFFFFu;
+    CellRange clamped(const Sizes& sz) const {
+        CellRange c = *this;
+        c.n_hi = c.n_hi < sz.n_neurons ? c.n_hi : sz.n_neurons;
+        c.a_hi = c.a_hi < sz.n_astro ? c.a_hi : sz.n_astro;
+        c.n_lo = c.n_lo < c.n_hi ? c.n_lo : c.n_hi;
+        c.a_lo = c.a_lo < c.a_hi ? c.a_lo : c.a_hi;
+        return c;
+    }
+    bool whole(const Sizes& sz) const {
+        const CellRange c = clamped(sz);
+        return c.n_lo == 0 && c.n_hi == sz.n_neurons && c.a_lo == 0 && c.a_hi == sz.n_astro;
+    }
+};
+
 struct Network {
     Network() = default;
     Network(Network&&) = default;
     Network& operator=(Network&&) = default;
     Sizes sz;
     u64 seed = 0;
+    CellRange own;  // clamped to sz; the CSRs below hold these cells' rows
     DeviceCSR exc, inh, sic, e2a;
+    // Edge counts of the whole network (exc, inh, e2a, sic), whatever `own` keeps.
+    u64 total_edges[4] = {0, 0, 0, 0};
+    bool partial() const { return !own.whole(sz); }
     // Per-cell parameters (src/astrosim_fused.cu:917-933), always double.
     DevBuf<double> Ca_tot, IP3_0, tau_IP3, delta_IP3, V_reset, b;
     double build_seconds = 0.0;
@@ -37,6 +64,8 @@ struct BuildOptions {
     // walked by one device thread (exact, no setup overhead); larger ones by the chunked
     // parallel builder.  0 forces the parallel builder, UINT64_MAX the sequential one.
     u64 sequential_max_draws = 50000ULL;
+    // Targets whose rows the network keeps (a rank of a sharded network: its cells).
+    CellRange own;
 };
 
 // Builds connectivity and per-cell parameters for (sizes, seed, biology) on `stream`,

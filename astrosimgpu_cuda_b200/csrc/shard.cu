@@ -435,7 +435,17 @@ Status ShardSim::create(const astrosim_config& cfg, const char* biology_json, in
     if (n < 1 || r < 0 || r >= n) return make_error(ASTROSIM_ERR_INVALID_ARG, "rank %d of %d", r, n);
     rank = r;
     world = n;
-    AS_TRY(sim.create(cfg, biology_json));
+    {
+        // this rank keeps the connectivity rows of its own cells only (about 1 / world of it)
+        const Sizes sz = scaling_law(cfg.n_total);
+        const ShardPlan pl = shard_plan(sz.n_neurons, sz.n_astro, r, n);
+        CellRange own;
+        own.n_lo = pl.n_lo;
+        own.n_hi = pl.n_hi;
+        own.a_lo = pl.a_lo;
+        own.a_hi = pl.a_hi;
+        AS_TRY(sim.create(cfg, biology_json, &own));
+    }
     if (!sim.windowed())
         return make_error(ASTROSIM_ERR_UNSUPPORTED,
                           "a sharded network needs the windowed engine (equal delays of 2-16 steps)");

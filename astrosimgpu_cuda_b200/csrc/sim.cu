@@ -126,7 +126,7 @@ Simulation::~Simulation() {
     }
 }
 
-Status Simulation::create(const astrosim_config& cfg, const char* biology_json) {
+Status Simulation::create(const astrosim_config& cfg, const char* biology_json, const CellRange* own) {
     if (cfg.n_total == 0) return make_error(ASTROSIM_ERR_INVALID_ARG, "n_total must be >= 1");
     if (!(cfg.dt > 0.0) || !std::isfinite(cfg.dt)) return make_error(ASTROSIM_ERR_INVALID_ARG, "dt must be > 0");
     if (cfg.substeps < 1) return make_error(ASTROSIM_ERR_INVALID_ARG, "substeps must be >= 1");
@@ -160,6 +160,7 @@ Status Simulation::create(const astrosim_config& cfg, const char* biology_json) 
     }
     const Sizes sz = scaling_law(cfg.n_total);
     BuildOptions bo;
+    if (own) bo.own = *own;
     AS_TRY(build_network(sz, cfg.seed, bio_, bo, net_, stream_));
 
     // run constants (src/astrosim_fused.cu:935-957, 1021-1024)
@@ -420,10 +421,10 @@ Status Simulation::summary(astrosim_summary_t& out) {
     out.n_inh = sz.n_inh;
     out.n_astro = sz.n_astro;
     out.p_primary = sz.p;
-    out.n_exc_edges = net_.exc.n_edges;
-    out.n_inh_edges = net_.inh.n_edges;
-    out.n_e2a_edges = net_.e2a.n_edges;
-    out.n_sic_edges = net_.sic.n_edges;
+    out.n_exc_edges = net_.total_edges[0];  // the whole network's, also on a rank that keeps part of it
+    out.n_inh_edges = net_.total_edges[1];
+    out.n_e2a_edges = net_.total_edges[2];
+    out.n_sic_edges = net_.total_edges[3];
     out.pre_steps = pre_steps_;
     out.sim_steps = sim_steps_;
     out.total_steps = total_steps_;
@@ -564,11 +565,12 @@ Status Simulation::dump_edges(const char* path) {
     std::ofstream out(path);
     if (!out) return make_error(ASTROSIM_ERR_IO, "cannot open %s for --dump-edges", path);
     out << "type,source,target\n";
-    struct Item { const DeviceCSR* c; const char* type; long long off; const char* sp; const char* tp; };
-    const Item items[4] = {{&net_.exc, "exc_primary", 0, "", ""},
-                           {&net_.inh, "inh_primary", static_cast<long long>(net_.sz.n_exc), "", ""},
-                           {&net_.e2a, "n2a", 0, "", "A"},
-                           {&net_.sic, "a2n", 0, "A", ""}};
+    // rows are the owned cells' (all of them unless this is a rank of a sharded network)
+    struct Item { const DeviceCSR* c; const char* type; long long off; const char* sp; const char* tp; u32 row0; };
+    const Item items[4] = {{&net_.exc, "exc_primary", 0, "", "", net_.own.n_lo},
+                           {&net_.inh, "inh_primary", static_cast<long long>(net_.sz.n_exc), "", "", net_.own.n_lo},
+                           {&net_.e2a, "n2a", 0, "", "A", net_.own.a_lo},
+                           {&net_.sic, "a2n", 0, "A", "", net_.own.n_lo}};
     std::vector<u32> rs, src;
     std::string buf;
     for (const Item& it : items) {
@@ -581,7 +583,7 @@ Status Simulation::dump_edges(const char* path) {
                 buf += std::to_string(static_cast<long long>(src[k]) + it.off);
                 buf += ',';
                 buf += it.tp;
-                buf += std::to_string(t);
+                buf += std::to_string(t + it.row0);
                 buf += '\n';
             }
             if (buf.size() > (1u << 22)) {

@@ -112,8 +112,10 @@ struct StateBuffers {
 
 class Simulation {
 public:
-    // biology_json: optional overrides of the biology constants (see apply_biology_json)
-    Status create(const astrosim_config& cfg, const char* biology_json = nullptr);
+    // biology_json: optional overrides of the biology constants (see apply_biology_json).
+    // own: the cells whose connectivity rows this network keeps (a rank of a sharded
+    // network); null keeps the whole network.  Only the owned cells may be stepped.
+    Status create(const astrosim_config& cfg, const char* biology_json = nullptr, const CellRange* own = nullptr);
     Status step(i64 n);
     Status summary(astrosim_summary_t& out);
     Status spike_counts(i64 first, i64 n, u32* dst);

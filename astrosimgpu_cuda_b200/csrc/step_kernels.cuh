@@ -384,13 +384,17 @@ inline StepPtrs<R> make_ptrs(StateBuffers& s, Network& n, const RunConsts& rc, i
     p.delta_IP3 = n.delta_IP3.get();
     p.V_reset = n.V_reset.get();
     p.b = n.b.get();
-    p.exc_rs = n.exc.row_start.get();
+    // The kernels index rows by cell id.  A network that keeps only the rows of its
+    // owned cells (a rank of a sharded network) stores row r for cell lo + r, so its
+    // row pointers are shifted back by lo; only owned cells are ever stepped, so only
+    // rows inside the arrays are read.  The shift is plain 64-bit address arithmetic.
+    p.exc_rs = n.exc.row_start.get() - n.own.n_lo;
     p.exc_src = n.exc.src.get();
-    p.inh_rs = n.inh.row_start.get();
+    p.inh_rs = n.inh.row_start.get() - n.own.n_lo;
     p.inh_src = n.inh.src.get();
-    p.sic_rs = n.sic.row_start.get();
+    p.sic_rs = n.sic.row_start.get() - n.own.n_lo;
     p.sic_src = n.sic.src.get();
-    p.e2a_rs = n.e2a.row_start.get();
+    p.e2a_rs = n.e2a.row_start.get() - n.own.a_lo;
     p.e2a_src = n.e2a.src.get();
     p.ca_rec = s.rec_n ? s.ca_rec.get() : nullptr;
     p.rec_every = s.rec_every;

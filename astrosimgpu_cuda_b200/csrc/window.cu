@@ -62,20 +62,27 @@ __global__ void lower_bound_rows_kernel(const u32* sorted_keys, u64 n, u32 n_row
     rs[t] = static_cast<u32>(lo);
 }
 
-__global__ void gather_fwd_kernel(const u32* edge_idx, u64 n, const u32* row_of_edge, const u32* tgt_rs, u32* dst,
-                                  u32* pos) {
+__global__ void gather_fwd_kernel(const u32* edge_idx, u64 n, const u32* row_of_edge, const u32* tgt_rs, u32 row0,
+                                  u32* dst, u32* pos) {
     const u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const u32 e = edge_idx[i];
     const u32 r = row_of_edge[e];
-    dst[i] = r;
+    dst[i] = r + row0;
     if (pos) pos[i] = e - tgt_rs[r];
+}
+
+__global__ void add_offset_kernel(u32* v, u64 n, u32 off) {
+    const u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) v[i] += off;
 }
 
 // Inverts a target-keyed CSR into a source-keyed one.  Within one source the
 // targets come out in increasing edge order (stable sort), which the push does not
-// depend on; positions let e2a deposits name their place in the target row.
-Status invert_csr(const DeviceCSR& c, u32 n_sources, DevBuf<u32>& rs, DevBuf<u32>& dst, DevBuf<u32>* pos,
+// depend on; positions let e2a deposits name their place in the target row.  Row r
+// of `c` is target row0 + r (a network that keeps only its owned cells' rows), and
+// the forward lists hold target ids.
+Status invert_csr(const DeviceCSR& c, u32 row0, u32 n_sources, DevBuf<u32>& rs, DevBuf<u32>& dst, DevBuf<u32>* pos,
                   cudaStream_t st) {
     const u64 n = c.n_edges;
     AS_TRY(rs.alloc(static_cast<size_t>(n_sources) + 1));
@@ -106,6 +113,7 @@ Status invert_csr(const DeviceCSR& c, u32 n_sources, DevBuf<u32>& rs, DevBuf<u32
                                                 n, 0, end_bit, st));
         lower_bound_rows_kernel<<<ceil_div(static_cast<u64>(n_sources) + 1, 256), 256, 0, st>>>(keys_out.get(), n,
                                                                                               n_sources, rs.get());
+        if (row0) add_offset_kernel<<<ceil_div(n, 256), 256, 0, st>>>(dst.get(), n, row0);
         AS_CUDA(cudaGetLastError());
         AS_CUDA(cudaStreamSynchronize(st));
         return Status::Ok();
@@ -123,8 +131,8 @@ Status invert_csr(const DeviceCSR& c, u32 n_sources, DevBuf<u32>& rs, DevBuf<u32
                                             0, end_bit, st));
     lower_bound_rows_kernel<<<ceil_div(static_cast<u64>(n_sources) + 1, 256), 256, 0, st>>>(keys_out.get(), n,
                                                                                           n_sources, rs.get());
-    gather_fwd_kernel<<<ceil_div(n, 256), 256, 0, st>>>(idx_out.get(), n, row_of.get(), c.row_start.get(), dst.get(),
-                                                        pos->get());
+    gather_fwd_kernel<<<ceil_div(n, 256), 256, 0, st>>>(idx_out.get(), n, row_of.get(), c.row_start.get(), row0,
+                                                        dst.get(), pos->get());
     AS_CUDA(cudaGetLastError());
     AS_CUDA(cudaStreamSynchronize(st));
     return Status::Ok();
@@ -137,9 +145,10 @@ Status window_setup(const RunConsts& rc, Network& net, bool fp32, WindowState& w
     const u64 nN = rc.n_neurons, nA = rc.n_astro;
     const size_t rb = fp32 ? sizeof(float) : sizeof(double);
     const size_t db = fp32 ? sizeof(Deposit<float>) : sizeof(Deposit<double>);
-    AS_TRY(invert_csr(net.exc, rc.n_exc, ws.fwd.exc_rs, ws.fwd.exc_dst, nullptr, st));
-    AS_TRY(invert_csr(net.inh, net.sz.n_inh, ws.fwd.inh_rs, ws.fwd.inh_dst, nullptr, st));
-    AS_TRY(invert_csr(net.e2a, rc.n_exc, ws.fwd.e2a_rs, ws.fwd.e2a_astro, &ws.fwd.e2a_pos, st));
+    // a rank of a sharded network keeps its own cells' rows: its forward lists reach its own cells only
+    AS_TRY(invert_csr(net.exc, net.own.n_lo, rc.n_exc, ws.fwd.exc_rs, ws.fwd.exc_dst, nullptr, st));
+    AS_TRY(invert_csr(net.inh, net.own.n_lo, net.sz.n_inh, ws.fwd.inh_rs, ws.fwd.inh_dst, nullptr, st));
+    AS_TRY(invert_csr(net.e2a, net.own.a_lo, rc.n_exc, ws.fwd.e2a_rs, ws.fwd.e2a_astro, &ws.fwd.e2a_pos, st));
     // Windows with more spikes than this use the pull gather instead of deposits.
     // ASTROSIM_PUSH_LIMIT overrides it (the tests force the pull path with 0).
     ws.push_limit = static_cast<u32>(std::max<u64>(1024, nN / 50));

@@ -42,12 +42,15 @@ def _lib():
         L.astrosim_shard_group_get_state.argtypes = [P, C.c_int, C.POINTER(C.c_double), C.c_size_t]
         L.astrosim_shard_group_spike_counts.argtypes = [P, C.c_int64, C.c_int64, u32p]
         L.astrosim_shard_group_destroy.argtypes = [P]
+        L.astrosim_shard_group_get_csr.argtypes = [P, C.c_int, C.c_int, u32p, C.c_size_t, u32p, C.c_size_t, u32p,
+                                                   u32p, C.POINTER(C.c_uint64)]
         for name in ("astrosim_shard_plan", "astrosim_shard_unique_id", "astrosim_shard_create",
                      "astrosim_shard_connect", "astrosim_shard_step", "astrosim_shard_summary",
                      "astrosim_shard_get_state", "astrosim_shard_spike_counts", "astrosim_shard_last_step_ms",
                      "astrosim_shard_destroy", "astrosim_shard_group_create", "astrosim_shard_group_step",
                      "astrosim_shard_group_summary", "astrosim_shard_group_get_state",
-                     "astrosim_shard_group_spike_counts", "astrosim_shard_group_destroy"):
+                     "astrosim_shard_group_spike_counts", "astrosim_shard_group_destroy",
+                     "astrosim_shard_group_get_csr"):
             getattr(L, name).restype = C.c_int
         _ARGS_SET = True
     return L
@@ -131,6 +134,17 @@ class ShardGroup:
         out = np.empty(n, dtype=np.uint32)
         check(_lib().astrosim_shard_group_spike_counts(self._h, first, n, _u32p(out)))
         return out
+
+    def csr(self, rank, name):
+        """(first_row, row_start, src) of CSR `name` as rank `rank` keeps it: the rows of its own cells."""
+        which = abi.CSR[name]
+        first, nr, ne = C.c_uint32(), C.c_uint32(), C.c_uint64()
+        f = _lib().astrosim_shard_group_get_csr
+        check(f(self._h, rank, which, None, 0, None, 0, C.byref(first), C.byref(nr), C.byref(ne)))
+        rs = np.empty(nr.value + 1, dtype=np.uint32)
+        src = np.empty(max(1, ne.value), dtype=np.uint32)
+        check(f(self._h, rank, which, _u32p(rs), rs.size, _u32p(src), src.size, None, None, None))
+        return first.value, rs, src[: ne.value]
 
 
 def agree_on_config(cfg, biology, group=None):

@@ -394,8 +394,10 @@ int astrosim_astro_totals_noalloc(const double* ca, const unsigned char* engaged
 
 /* ------------------------------------------------------------------ one network on several GPUs
  * A network split across `world` ranks (the reference
- * runs on one GPU).  Every rank builds the whole network and owns contiguous
- * ranges of neurons and astrocytes (128-cell blocks, balanced); per 1 ms window
+ * runs on one GPU).  Every rank owns contiguous ranges of neurons and astrocytes
+ * (128-cell blocks, balanced) and builds and keeps only the connectivity rows of
+ * its own cells (about 1 / world of the connectivity; the build walks the whole
+ * deterministic stream but emits only those rows); per 1 ms window
  * it advances its own cells, then the ranks all-gather the window's spikes and the
  * SIC factors of their active astrocytes, and each rank delivers every spike into
  * its own cells.  Results (spike counts, raster, every state array, the summary)
@@ -455,6 +457,13 @@ int astrosim_shard_group_step(astrosim_shard_group* g, int64_t n_steps);
 int astrosim_shard_group_summary(astrosim_shard_group* g, astrosim_summary_t* out);
 int astrosim_shard_group_get_state(astrosim_shard_group* g, int which, double* dst, size_t count);
 int astrosim_shard_group_spike_counts(astrosim_shard_group* g, int64_t first_step, int64_t n, uint32_t* counts);
+/* The connectivity rank `rank` keeps: CSR `which` (ASTROSIM_CSR_*) restricted to the
+   rank's own targets, row r being cell *first_row + r (neurons for exc/inh/sic,
+   astrocytes for e2a).  Each rank keeps only these rows, about 1 / world of the
+   network; every kept row equals the whole network's row.  Sizes as astrosim_get_csr. */
+int astrosim_shard_group_get_csr(astrosim_shard_group* g, int rank, int which, uint32_t* row_start, size_t row_cap,
+                                 uint32_t* src, size_t src_cap, uint32_t* first_row, uint32_t* n_rows,
+                                 uint64_t* n_edges);
 int astrosim_shard_group_destroy(astrosim_shard_group* g);
 
 /*

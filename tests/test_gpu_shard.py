@@ -42,6 +42,39 @@ def test_group_matches_single_gpu(world, precision, n_total):
             compare(g, s, f"w{world} {precision} N{n_total} after {chunk}")
 
 
+@pytest.mark.parametrize("n_total,builder", [(20000, None), (3000, "sequential")])
+def test_each_rank_keeps_only_its_own_rows(monkeypatch, n_total, builder):
+    """A rank builds and keeps the connectivity rows of its own cells only (the chunked
+    builder emits just those edges; the one-thread walk for small networks slices its
+    CSRs), about 1 / world of the network; every kept row is the whole network's row,
+    and the summary still reports the whole network's edge counts."""
+    if builder:
+        monkeypatch.setenv("ASTROSIM_BUILDER", builder)
+    world = 3
+    kw = dict(n_total=n_total, seed=11, pre_ms=0.0, sim_ms=1.0)
+    with shard.ShardGroup(world=world, **kw) as g, asg.Simulation(**kw) as s:
+        for name in ("exc", "inh", "sic", "e2a"):
+            rs_full, src_full = s.csr(name)
+            held = 0
+            next_row = 0
+            for r in range(world):
+                first, rs, src = g.csr(r, name)
+                plan = shard.shard_plan(n_total, r, world)
+                assert first == (plan[2] if name == "e2a" else plan[0])
+                assert first == next_row
+                lo, hi = first, first + rs.size - 1
+                next_row = hi
+                np.testing.assert_array_equal(rs, rs_full[lo:hi + 1] - rs_full[lo], err_msg=f"{name} rank {r}")
+                np.testing.assert_array_equal(src, src_full[rs_full[lo]:rs_full[hi]], err_msg=f"{name} rank {r}")
+                held += src.size
+                assert src.size <= 1.25 * src_full.size / world + 64, (name, r, src.size, src_full.size)
+            assert next_row == rs_full.size - 1
+            assert held == src_full.size
+        a, b = g.summary(), s.summary()
+        for k in ("n_exc_edges", "n_inh_edges", "n_e2a_edges", "n_sic_edges"):
+            assert a[k] == b[k], k
+
+
 def test_group_busy_windows_and_raster():
     # a strong drive makes most windows busy (pull delivery) early on
     bio = {"exc_poiss_rate": 27000.0, "inh_poiss_rate": 25000.0}
@@ -83,3 +116,28 @@ def test_one_rank_per_process_world_of_one(tmp_path):
             assert r.last_step_ms() > 0
     finally:
         dist.destroy_process_group()
+
+
+def test_group_at_full_size_keeps_half_the_rows_each():
+    """N_total = 1e7 split over two ranks (both on this GPU, one after another): each
+    rank keeps about half of the 1.32e9 connectivity rows, and 20 windows give the
+    single-GPU run's results bit for bit."""
+    kw = dict(n_total=10_000_000, seed=1, pre_ms=0.0, sim_ms=20.0, precision="fp32")
+    with asg.Simulation(**kw) as s:
+        s.step(200)
+        want = {name: s.state(name) for name in ("V", "w", "g_ex", "Ca", "IP3", "h", "sic_factor")}
+        want_counts = s.spike_counts()
+        want_summary = s.summary()
+    with shard.ShardGroup(world=2, **kw) as g:
+        held = []
+        for r in range(2):
+            held.append(sum(g.csr(r, name)[2].size for name in ("exc", "inh", "sic", "e2a")))
+        total = sum(want_summary[k] for k in ("n_exc_edges", "n_inh_edges", "n_e2a_edges", "n_sic_edges"))
+        assert sum(held) == total
+        for h in held:
+            assert abs(h - total / 2) <= 0.02 * total, (h, total)
+        g.step(200)
+        np.testing.assert_array_equal(g.spike_counts(), want_counts)
+        for name, v in want.items():
+            np.testing.assert_array_equal(g.state(name), v, err_msg=name)
+        assert want_counts.sum() > 0
