@@ -153,7 +153,25 @@ struct Bio {
 struct NeuronP {  // src/astrosim_fused.cu:228-232
     double C_m, g_L, E_L, V_th, Delta_T, a, tau_w, V_peak, t_ref, E_ex, E_in, tau_syn_ex, tau_syn_in,
         I_e, psc_ex, psc_in;
+    // Test knob (oracle_set_exp_perturbation): the fraction of the AdEx exponential's
+    // arguments whose result is moved by one ulp; 0 evaluates the plain formula.
+    double exp_perturb = 0.0;
 };
+
+// exp(x), moved one ulp up or down for a fraction `rate` of the arguments (chosen by a
+// hash of x's bits, so the same argument always gets the same result): a stand-in for
+// another correctly working math library that disagrees with this one in the last bit.
+inline double exp_maybe_perturbed(double x, double rate) {
+    const double r = std::exp(x);
+    if (rate <= 0.0) return r;
+    u64 z = 0;
+    std::memcpy(&z, &x, sizeof z);
+    z = (z ^ (z >> 33)) * 0xFF51AFD7ED558CCDULL;
+    z = (z ^ (z >> 33)) * 0xC4CEB9FE1A85EC53ULL;
+    z ^= z >> 33;
+    if (static_cast<double>(z >> 11) * (1.0 / 9007199254740992.0) >= rate) return r;
+    return std::nextafter(r, (z & 1) ? HUGE_VAL : -HUGE_VAL);
+}
 NeuronP make_neuron(bool exc, const Bio& b) {  // src/astrosim_fused.cu:940-951
     NeuronP p{};
     p.C_m = exc ? b.e_C_m : b.i_C_m;
@@ -440,7 +458,7 @@ inline void astro_rhs(const Bio& c, double Ca_tot, double IP3_0, double tau_IP3,
 inline void neuron_rhs(const NeuronP& p, double V, double w, double g_ex, double g_in, double I_ext,
                        double& dV, double& dw) {
     const double Vc = V < p.V_peak ? V : p.V_peak;
-    const double I_spike = p.g_L * p.Delta_T * std::exp((Vc - p.V_th) / p.Delta_T);
+    const double I_spike = p.g_L * p.Delta_T * exp_maybe_perturbed((Vc - p.V_th) / p.Delta_T, p.exp_perturb);
     const double I_syn_ex = g_ex * (Vc - p.E_ex);
     const double I_syn_in = g_in * (Vc - p.E_in);
     dV = (-p.g_L * (Vc - p.E_L) + I_spike - I_syn_ex - I_syn_in - w + p.I_e + I_ext) / p.C_m;
@@ -845,5 +863,11 @@ int oracle_raster(oracle_sim* s, uint32_t* bits_out, size_t words) {
 }
 
 double oracle_build_seconds(oracle_sim* s) { return s->build_s; }
+
+void oracle_set_exp_perturbation(oracle_sim* s, double rate) {
+    if (!s) return;
+    s->pe.exp_perturb = rate;
+    s->pi.exp_perturb = rate;
+}
 
 }  // extern "C"

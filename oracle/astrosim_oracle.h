@@ -81,6 +81,14 @@ int oracle_raster(oracle_sim* s, uint32_t* bits, size_t words);
 /* Seconds spent in oracle_create's connectivity build. */
 double oracle_build_seconds(oracle_sim* s);
 
+/*
+ * Sensitivity probe: from now on, the AdEx exponential (src/astrosim_fused.cu:286)
+ * returns a result one ulp away from the host C library's for a fraction `rate` of
+ * its arguments (chosen by a hash of the argument, so deterministic), standing in
+ * for a second correct math library that disagrees in the last bit.  0 turns it off.
+ */
+void oracle_set_exp_perturbation(oracle_sim* s, double rate);
+
 #ifdef __cplusplus
 }
 #endif

@@ -58,6 +58,7 @@ def lib():
         L.oracle_raster.argtypes = [P, u32p, C.c_size_t]
         L.oracle_build_seconds.restype = C.c_double
         L.oracle_build_seconds.argtypes = [P]
+        L.oracle_set_exp_perturbation.argtypes = [P, C.c_double]
         _lib = L
     return _lib
 
@@ -122,6 +123,10 @@ class OracleSim:
 
     def __del__(self):
         self.close()
+
+    def perturb_exp(self, rate):
+        """Moves the AdEx exponential one ulp for a fraction `rate` of its arguments (0: off)."""
+        lib().oracle_set_exp_perturbation(self._h, float(rate))
 
     def step(self, n):
         lib().oracle_step(self._h, n)
