@@ -3,8 +3,10 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <cstdlib>
 #include <cstring>
 #include <thread>
+#include <type_traits>
 
 #include "ensemble.cuh"
 #include "window_kernels.cuh"
@@ -21,17 +23,29 @@ struct alignas(16) NetDesc {
     i64 mark;  // last step of the pre-run (src/astrosim_fused.cu:1066)
 };
 
-constexpr int kEnsVariants[] = {6, 8, 4};  // launch-bounds minimum blocks, as the single-network engine
-constexpr int kEnsNumVariants = 3;
+// Variants the autotuner chooses from: (tile size = block size, minimum resident
+// blocks per SM).  A tile is `tile` consecutive cells of one population of one
+// network; each block stages its network's descriptor once, so larger tiles stage
+// less per cell and smaller tiles balance networks of very different sizes better.
+struct EnsVariant {
+    int tile, min_blocks;
+};
+constexpr EnsVariant kEnsVariantsF32[] = {{128, 6}, {128, 8}, {128, 4}, {64, 12}, {64, 16}, {64, 8},
+                                          {256, 3}, {256, 4}, {256, 2}};
+constexpr EnsVariant kEnsVariantsF64[] = {{128, 4}, {128, 5}, {128, 3}, {64, 8}, {64, 10}, {64, 6},
+                                          {256, 2}, {256, 3}, {256, 1}};
+constexpr int kEnsNumVariants = 9;
+constexpr int kTileSizes[kNumTileSizes] = {64, 128, 256};
+int tile_index(int tile) { return tile == 64 ? 0 : (tile == 256 ? 2 : 1); }
 constexpr int kEnsTuneRounds = 2;
 constexpr int kGraphWindows = 10;
 constexpr u32 kPushBlocksPerNet = 4;
 
-// One window of one 128-cell tile.  UNI: every network shares the constants outside
-// NetScalars, which then come from the kernel parameters (`common`); otherwise each
-// block also stages its network's full constants (`rcs`) into shared memory.
-template <typename R, int MB, bool UNI>
-__global__ void __launch_bounds__(128, MB) ens_window_kernel(RunConsts common, const RunConsts* __restrict__ rcs,
+// One window of one tile of blockDim.x cells.  UNI: every network shares the constants
+// outside NetScalars, which then come from the kernel parameters (`common`); otherwise
+// each block also stages its network's full constants (`rcs`) into shared memory.
+template <typename R, int TILE, int MB, bool UNI>
+__global__ void __launch_bounds__(TILE, MB) ens_window_kernel(RunConsts common, const RunConsts* __restrict__ rcs,
                                                              const NetDesc<R>* __restrict__ descs,
                                                              const u32* __restrict__ tile_net,
                                                              const u32* __restrict__ tile_blk,
@@ -89,12 +103,38 @@ __global__ void ens_advance_kernel(i64* win, const i64* stop, u32 n, int W) {
 template <typename R, bool UNI>
 void launch_ens_window_v(int v, u32 grid, cudaStream_t st, const RunConsts& common, const RunConsts* rcs,
                          const NetDesc<R>* d, const u32* tn, const u32* tb, const i64* win, const i64* stop, int W) {
-    switch (kEnsVariants[v]) {
-        case 4: ens_window_kernel<R, 4, UNI><<<grid, 128, 0, st>>>(common, rcs, d, tn, tb, win, stop, W); break;
-        case 8: ens_window_kernel<R, 8, UNI><<<grid, 128, 0, st>>>(common, rcs, d, tn, tb, win, stop, W); break;
-        default: ens_window_kernel<R, 6, UNI><<<grid, 128, 0, st>>>(common, rcs, d, tn, tb, win, stop, W); break;
+    constexpr bool f32 = std::is_same<R, float>::value;
+    const EnsVariant x = f32 ? kEnsVariantsF32[v] : kEnsVariantsF64[v];
+#define AS_ENS(T, M) ens_window_kernel<R, T, M, UNI><<<grid, T, 0, st>>>(common, rcs, d, tn, tb, win, stop, W)
+    if constexpr (f32) {
+        switch (x.tile * 100 + x.min_blocks) {
+            case 12808: AS_ENS(128, 8); break;
+            case 12804: AS_ENS(128, 4); break;
+            case 6412: AS_ENS(64, 12); break;
+            case 6416: AS_ENS(64, 16); break;
+            case 6408: AS_ENS(64, 8); break;
+            case 25603: AS_ENS(256, 3); break;
+            case 25604: AS_ENS(256, 4); break;
+            case 25602: AS_ENS(256, 2); break;
+            default: AS_ENS(128, 6); break;
+        }
+    } else {
+        switch (x.tile * 100 + x.min_blocks) {
+            case 12805: AS_ENS(128, 5); break;
+            case 12803: AS_ENS(128, 3); break;
+            case 6408: AS_ENS(64, 8); break;
+            case 6410: AS_ENS(64, 10); break;
+            case 6406: AS_ENS(64, 6); break;
+            case 25602: AS_ENS(256, 2); break;
+            case 25603: AS_ENS(256, 3); break;
+            case 25601: AS_ENS(256, 1); break;
+            default: AS_ENS(128, 4); break;
+        }
     }
+#undef AS_ENS
 }
+
+int variant_tile(bool fp32, int v) { return fp32 ? kEnsVariantsF32[v].tile : kEnsVariantsF64[v].tile; }
 
 // One window and its push for every network.
 template <typename R>
@@ -170,8 +210,10 @@ Ensemble::~Ensemble() {
     nets_.clear();
     descs_.release();
     rcs_.release();
-    tile_net_.release();
-    tile_blk_.release();
+    for (int ti = 0; ti < kNumTileSizes; ++ti) {
+        tile_net_[ti].release();
+        tile_blk_[ti].release();
+    }
     win_.release();
     stop_.release();
     if (stream_) {
@@ -245,27 +287,33 @@ Status Ensemble::rebuild() {
     AllocStream alloc_scope(stream_);
     if (fp32_) AS_TRY(build_descs<float>(nets_, descs_, rcs_, common_, uniform_, stream_));
     else AS_TRY(build_descs<double>(nets_, descs_, rcs_, common_, uniform_, stream_));
-    std::vector<u32> tn, tb;
-    for (u32 i = 0; i < nets_.size(); ++i) {
-        if (!nets_[i]) continue;
-        const RunConsts& rc = nets_[i]->consts();
-        for (u32 b = 0; b < ceil_div(rc.n_astro, 128); ++b) {
-            tn.push_back(i);
-            tb.push_back(b | 0x80000000u);
+    // one tile table per tile size: tile b of a population covers its cells [b * tile, (b + 1) * tile)
+    for (int ti = 0; ti < kNumTileSizes; ++ti) {
+        const u32 tile = static_cast<u32>(kTileSizes[ti]);
+        std::vector<u32> tn, tb;
+        for (u32 i = 0; i < nets_.size(); ++i) {
+            if (!nets_[i]) continue;
+            const RunConsts& rc = nets_[i]->consts();
+            for (u32 b = 0; b < ceil_div(rc.n_astro, tile); ++b) {
+                tn.push_back(i);
+                tb.push_back(b | 0x80000000u);
+            }
+            for (u32 b = 0; b < ceil_div(rc.n_neurons, tile); ++b) {
+                tn.push_back(i);
+                tb.push_back(b);
+            }
         }
-        for (u32 b = 0; b < ceil_div(rc.n_neurons, 128); ++b) {
-            tn.push_back(i);
-            tb.push_back(b);
+        n_tiles_[ti] = static_cast<u32>(tn.size());
+        AS_TRY(tile_net_[ti].alloc(std::max<size_t>(1, tn.size())));
+        AS_TRY(tile_blk_[ti].alloc(std::max<size_t>(1, tb.size())));
+        if (!tn.empty()) {
+            AS_CUDA(cudaMemcpyAsync(tile_net_[ti].get(), tn.data(), tn.size() * sizeof(u32), cudaMemcpyHostToDevice,
+                                    stream_));
+            AS_CUDA(cudaMemcpyAsync(tile_blk_[ti].get(), tb.data(), tb.size() * sizeof(u32), cudaMemcpyHostToDevice,
+                                    stream_));
         }
+        AS_CUDA(cudaStreamSynchronize(stream_));  // the host vectors die at the end of this iteration
     }
-    n_tiles_ = static_cast<u32>(tn.size());
-    AS_TRY(tile_net_.alloc(std::max<size_t>(1, tn.size())));
-    AS_TRY(tile_blk_.alloc(std::max<size_t>(1, tb.size())));
-    if (!tn.empty()) {
-        AS_CUDA(cudaMemcpyAsync(tile_net_.get(), tn.data(), tn.size() * sizeof(u32), cudaMemcpyHostToDevice, stream_));
-        AS_CUDA(cudaMemcpyAsync(tile_blk_.get(), tb.data(), tb.size() * sizeof(u32), cudaMemcpyHostToDevice, stream_));
-    }
-    AS_CUDA(cudaStreamSynchronize(stream_));
     if (graph_) {
         cudaGraphExecDestroy(graph_);
         graph_ = nullptr;
@@ -276,12 +324,13 @@ Status Ensemble::rebuild() {
 
 void Ensemble::launch_window(int v) {
     const u32 n = static_cast<u32>(nets_.size());
+    const int ti = tile_index(variant_tile(fp32_, v));
     if (fp32_)
-        launch_ens_window<float>(v, uniform_, n_tiles_, n, stream_, common_, rcs_.get(), descs_.get(), tile_net_.get(),
-                                 tile_blk_.get(), win_.get(), stop_.get(), W_);
+        launch_ens_window<float>(v, uniform_, n_tiles_[ti], n, stream_, common_, rcs_.get(), descs_.get(),
+                                 tile_net_[ti].get(), tile_blk_[ti].get(), win_.get(), stop_.get(), W_);
     else
-        launch_ens_window<double>(v, uniform_, n_tiles_, n, stream_, common_, rcs_.get(), descs_.get(),
-                                  tile_net_.get(), tile_blk_.get(), win_.get(), stop_.get(), W_);
+        launch_ens_window<double>(v, uniform_, n_tiles_[ti], n, stream_, common_, rcs_.get(), descs_.get(),
+                                  tile_net_[ti].get(), tile_blk_[ti].get(), win_.get(), stop_.get(), W_);
 }
 
 Status Ensemble::capture_graph() {
@@ -312,7 +361,7 @@ Status Ensemble::advance_windows(i64 windows) {
     AS_CUDA(cudaSetDevice(device_));
     if (dirty_) AS_TRY(rebuild());
     const u32 n = static_cast<u32>(nets_.size());
-    if (n == 0 || n_tiles_ == 0 || windows <= 0) return Status::Ok();
+    if (n == 0 || n_tiles_[1] == 0 || windows <= 0) return Status::Ok();
     const auto t0 = std::chrono::steady_clock::now();
     AS_CUDA(cudaEventRecord(ev0_, stream_));
     i64 done = 0;
@@ -322,7 +371,12 @@ Status Ensemble::advance_windows(i64 windows) {
         AS_CUDA(cudaGetLastError());
         return Status::Ok();
     };
-    // autotune the launch-bounds variant on the first windows (results do not depend on it)
+    // autotune the (tile size, launch bounds) variant on the first windows (results do not
+    // depend on it); ASTROSIM_ENSEMBLE_VARIANT fixes it (the tests run every variant)
+    if (variant_ < 0) {
+        if (const char* env = std::getenv("ASTROSIM_ENSEMBLE_VARIANT"))
+            variant_ = std::min(kEnsNumVariants - 1, std::max(0, std::atoi(env)));
+    }
     while (variant_ < 0 && done < windows) {
         const int v = tune_step_ % kEnsNumVariants;
         cudaEvent_t a = nullptr, b = nullptr;

@@ -2,7 +2,8 @@
 //
 // Each network keeps its own device state exactly as a single Simulation (its own
 // windowed engine buffers).  One window launch covers every cell of every network:
-// a tile table maps each 128-cell block to (network, population, block), and each
+// a tile table maps each block (a tile of 64, 128 or 256 cells: the autotuner times
+// each size with three occupancy targets) to (network, population, tile), and each
 // block reads its network's descriptor (constants and pointers) into shared memory.
 // The constants that differ between networks (NetScalars) sit in the descriptor;
 // when every network shares the rest (the same biology, dt and substeps) those come
@@ -19,6 +20,8 @@
 #include "sim.cuh"
 
 namespace astrosim {
+
+constexpr int kNumTileSizes = 3;  // tiles of 64, 128 or 256 cells, chosen by the autotuner
 
 class Ensemble {
 public:
@@ -62,13 +65,14 @@ private:
     DevBuf<unsigned char> rcs_;  // RunConsts per network (read when !uniform_)
     RunConsts common_{};         // shared constants (NetScalars fields cleared)
     bool uniform_ = true;
-    DevBuf<u32> tile_net_, tile_blk_;
+    // tile tables for tiles of 64, 128 and 256 cells
+    DevBuf<u32> tile_net_[kNumTileSizes], tile_blk_[kNumTileSizes];
     DevBuf<i64> win_, stop_;
-    u32 n_tiles_ = 0;
+    u32 n_tiles_[kNumTileSizes] = {0, 0, 0};
     bool dirty_ = true;
-    int variant_ = -1;
+    int variant_ = -1;  // (tile size, launch bounds) variant; -1 while the autotuner times them
     int tune_step_ = 0;
-    float tune_ms_[4] = {1e30f, 1e30f, 1e30f, 1e30f};
+    float tune_ms_[9] = {1e30f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f};
     cudaGraphExec_t graph_ = nullptr;
     int graph_windows_ = 0;
     i64 steps_done_ = 0;

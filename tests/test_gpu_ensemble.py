@@ -82,3 +82,26 @@ def test_ensemble_rejects_mixed_precision_and_partial_windows():
     with asg.Ensemble([a, a]) as ens:
         with pytest.raises(asg.AstrosimError):
             ens.step(7)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_every_tile_shape_is_bit_identical(monkeypatch, precision):
+    """The autotuner picks a (tile size, occupancy) pair: tiles of 64, 128 or 256 cells
+    with three launch-bounds targets each.  Every pair gives each network the result
+    of running it alone."""
+    cfgs = [abi.default_config(n_total=n, seed=70 + i, pre_ms=5.0, sim_ms=35.0, precision=precision)
+            for i, n in enumerate((700, 3300, 9000))]
+    solo = []
+    for cfg in cfgs:
+        with asg.Simulation(cfg) as sim:
+            sim.step(sim.summary()["total_steps"])
+            solo.append(({k: sim.state(k) for k in STATES}, sim.spike_counts()))
+    for v in range(9):
+        monkeypatch.setenv("ASTROSIM_ENSEMBLE_VARIANT", str(v))
+        with asg.Ensemble(cfgs) as ens:
+            ens.step(400)
+            for i in range(len(cfgs)):
+                np.testing.assert_array_equal(ens.spike_counts(i), solo[i][1], err_msg=f"variant {v} net {i}")
+                for k in STATES:
+                    np.testing.assert_array_equal(ens.state(i, k), solo[i][0][k], err_msg=f"variant {v} net {i} {k}")
+    monkeypatch.delenv("ASTROSIM_ENSEMBLE_VARIANT")
