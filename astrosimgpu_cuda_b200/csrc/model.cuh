@@ -385,6 +385,12 @@ __device__ __forceinline__ void astro_rhs(const AstroK& c, double Ca_tot, double
 __device__ __forceinline__ double exp_r(double x) { return exp(x); }
 __device__ __forceinline__ float exp_r(float x) { return expf(x); }
 
+// CUDA's double exp, kept out of line: inlined four times per RK4 step its expansion
+// needs about 50 more registers than the rest of the step, which made the FP64 window
+// kernel spill at every occupancy above 3 blocks per SM.  It is the same function, so
+// the results are unchanged.
+static __device__ __noinline__ double exp_outlined(double x) { return exp(x); }
+
 // AdEx: src/astrosim_fused.cu:281-290 (operand order kept; the divisions by the
 // constants C_m, tau_w and Delta_T are exact, see div_by).
 __device__ __forceinline__ void neuron_rhs(const NeuronK& p, double V, double w, double g_ex, double g_in,
@@ -392,7 +398,7 @@ __device__ __forceinline__ void neuron_rhs(const NeuronK& p, double V, double w,
     const double Vc = V < p.V_peak ? V : p.V_peak;
     const double arg = p.inv_Delta_T_pow2 != 0.0 ? (Vc - p.V_th) * p.inv_Delta_T_pow2
                                                  : div_by(Vc - p.V_th, p.Delta_T, p.rcp_Delta_T);
-    const double I_spike = p.g_L * p.Delta_T * exp(arg);
+    const double I_spike = p.g_L * p.Delta_T * exp_outlined(arg);
     const double I_syn_ex = g_ex * (Vc - p.E_ex);
     const double I_syn_in = g_in * (Vc - p.E_in);
     dV = div_by(-p.g_L * (Vc - p.E_L) + I_spike - I_syn_ex - I_syn_in - w + p.I_e + I_ext, p.C_m, p.rcp_C_m);
