@@ -91,26 +91,59 @@ __device__ __forceinline__ u32 skip_at(const Sec& s, u64 t) {
     return __ldg(s.cache + i);
 }
 
+// The skip at tape position t, loaded ahead of knowing whether the walk draws it
+// (no error flag; the draw itself goes through skip_checked).
+__device__ __forceinline__ u32 skip_peek(const Sec& s, u64 t) {
+    const u64 i = t - s.cache_base;
+    return i < s.cache_len ? __ldg(s.cache + i) : 0xFFFFFFFFu;
+}
+
+// Draws the skip at position t whose value was peeked: skip_at(s, t) without the load.
+__device__ __forceinline__ u32 skip_checked(const Sec& s, u64 t, u32 peeked) {
+    if (t - s.cache_base >= s.cache_len) {
+        atomicOr(s.err, kErrCache);
+        return 0xFFFFFFFFu;
+    }
+    return peeked;
+}
+
+// The third-factor test u < P_THIRD (src/astrosim_fused.cu:699) on the 53-bit integer m
+// of u = m * 2^-53: u < P_THIRD exactly when m < kThirdLim = ceil(P_THIRD * 2^53)
+// (the product is exact, a power-of-two scaling).
+constexpr double kThirdScaled = kPThird * 9007199254740992.0;
+constexpr u64 kThirdLim = static_cast<u64>(kThirdScaled) +
+                          (static_cast<double>(static_cast<u64>(kThirdScaled)) < kThirdScaled ? 1u : 0u);
+
 struct NoVisit {
     __device__ __forceinline__ void operator()(u32, bool, u32) const {}
 };
 
 // One pre's walk from tape position c (src/astrosim_fused.cu:688-707, 712-723).
 // A landing on `self_post` is an autapse: no edge and no third-factor draws.
-// Returns the tape position after the walk.
+// Returns the tape position after the walk.  The draws and their order are the
+// reference's; each post's next skip is loaded before its third-factor draws are
+// hashed (both possible positions when the post has a third-factor test), so the
+// cache load and the hash overlap instead of following each other.
 template <class V>
 __device__ __forceinline__ u64 walk_pre(const Sec& s, u64 c, u32 self_post, V& visit) {
     u32 pos = 0;
     const u32 n = s.post_count;
-    while (pos < n) {
-        const u32 g = skip_at(s, c++);
+    if (n == 0) return c;
+    u32 g = skip_at(s, c++);
+    for (;;) {
         if (g >= n - pos) break;  // the skip reaches the end of the block
         pos += g;
         const u32 post = s.post_off + pos;
         ++pos;
-        if (post == self_post) continue;
+        const bool more = pos < n;  // another skip is drawn after this post
+        if (post == self_post) {
+            if (!more) break;
+            g = skip_at(s, c++);
+            continue;
+        }
         if (s.third) {
-            const bool hit = !(rng_uniform(s.seed, kSetupStream, c++) >= kPThird);
+            const u32 g_miss = skip_peek(s, c + 1), g_hit = skip_peek(s, c + 2);
+            const bool hit = (rng_bits(s.seed, kSetupStream, c++) >> 11) < kThirdLim;
             u32 astro = 0;
             if (hit) {
                 const double u = rng_uniform(s.seed, kSetupStream, c++);
@@ -118,8 +151,15 @@ __device__ __forceinline__ u64 walk_pre(const Sec& s, u64 c, u32 self_post, V& v
                                static_cast<u32>(static_cast<u64>(u * static_cast<double>(s.take)) % s.take)];
             }
             visit(post, hit, astro);
+            if (!more) break;
+            g = skip_checked(s, c, hit ? g_hit : g_miss);
+            ++c;
         } else {
+            const u32 g_next = skip_peek(s, c);
             visit(post, false, 0u);
+            if (!more) break;
+            g = skip_checked(s, c, g_next);
+            ++c;
         }
     }
     return c;
