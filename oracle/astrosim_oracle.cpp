@@ -156,6 +156,9 @@ struct NeuronP {  // src/astrosim_fused.cu:228-232
     // Test knob (oracle_set_exp_perturbation): the fraction of the AdEx exponential's
     // arguments whose result is moved by one ulp; 0 evaluates the plain formula.
     double exp_perturb = 0.0;
+    // Test knob (oracle_set_contraction): evaluate the AdEx right-hand side and the
+    // neuron's RK4 updates with fused multiply-adds, as a GPU compiler contracts them.
+    bool contract = false;
 };
 
 // exp(x), moved one ulp up or down for a fraction `rate` of the arguments (chosen by a
@@ -459,6 +462,14 @@ inline void neuron_rhs(const NeuronP& p, double V, double w, double g_ex, double
                        double& dV, double& dw) {
     const double Vc = V < p.V_peak ? V : p.V_peak;
     const double I_spike = p.g_L * p.Delta_T * exp_maybe_perturbed((Vc - p.V_th) / p.Delta_T, p.exp_perturb);
+    if (p.contract) {  // the same expression with each product fused into the sum that uses it
+        double t = std::fma(-p.g_L, Vc - p.E_L, I_spike);
+        t = std::fma(-g_ex, Vc - p.E_ex, t);
+        t = std::fma(-g_in, Vc - p.E_in, t);
+        dV = (t - w + p.I_e + I_ext) / p.C_m;
+        dw = std::fma(p.a, Vc - p.E_L, -w) / p.tau_w;
+        return;
+    }
     const double I_syn_ex = g_ex * (Vc - p.E_ex);
     const double I_syn_in = g_in * (Vc - p.E_in);
     dV = (-p.g_L * (Vc - p.E_L) + I_spike - I_syn_ex - I_syn_in - w + p.I_e + I_ext) / p.C_m;
@@ -580,12 +591,22 @@ int neuron_cell(oracle_sim* s, u32 j, int64_t step, bool sic_refresh, u64 noise_
             const double g_ex_mid = 0.5 * (g_ex + g_ex_next);
             const double g_in_mid = 0.5 * (g_in + g_in_next);
             double k1V, k1w, k2V, k2w, k3V, k3w, k4V, k4w;
-            neuron_rhs(p, V, w, g_ex, g_in, I_ext, k1V, k1w);
-            neuron_rhs(p, V + 0.5 * hs * k1V, w + 0.5 * hs * k1w, g_ex_mid, g_in_mid, I_ext, k2V, k2w);
-            neuron_rhs(p, V + 0.5 * hs * k2V, w + 0.5 * hs * k2w, g_ex_mid, g_in_mid, I_ext, k3V, k3w);
-            neuron_rhs(p, V + hs * k3V, w + hs * k3w, g_ex_next, g_in_next, I_ext, k4V, k4w);
-            V += (hs / 6.0) * (k1V + 2.0 * k2V + 2.0 * k3V + k4V);
-            w += (hs / 6.0) * (k1w + 2.0 * k2w + 2.0 * k3w + k4w);
+            if (p.contract) {  // stage arguments and the weighted sum with fused multiply-adds
+                const double hh = 0.5 * hs;
+                neuron_rhs(p, V, w, g_ex, g_in, I_ext, k1V, k1w);
+                neuron_rhs(p, std::fma(hh, k1V, V), std::fma(hh, k1w, w), g_ex_mid, g_in_mid, I_ext, k2V, k2w);
+                neuron_rhs(p, std::fma(hh, k2V, V), std::fma(hh, k2w, w), g_ex_mid, g_in_mid, I_ext, k3V, k3w);
+                neuron_rhs(p, std::fma(hs, k3V, V), std::fma(hs, k3w, w), g_ex_next, g_in_next, I_ext, k4V, k4w);
+                V = std::fma(hs / 6.0, std::fma(2.0, k3V, std::fma(2.0, k2V, k1V)) + k4V, V);
+                w = std::fma(hs / 6.0, std::fma(2.0, k3w, std::fma(2.0, k2w, k1w)) + k4w, w);
+            } else {
+                neuron_rhs(p, V, w, g_ex, g_in, I_ext, k1V, k1w);
+                neuron_rhs(p, V + 0.5 * hs * k1V, w + 0.5 * hs * k1w, g_ex_mid, g_in_mid, I_ext, k2V, k2w);
+                neuron_rhs(p, V + 0.5 * hs * k2V, w + 0.5 * hs * k2w, g_ex_mid, g_in_mid, I_ext, k3V, k3w);
+                neuron_rhs(p, V + hs * k3V, w + hs * k3w, g_ex_next, g_in_next, I_ext, k4V, k4w);
+                V += (hs / 6.0) * (k1V + 2.0 * k2V + 2.0 * k3V + k4V);
+                w += (hs / 6.0) * (k1w + 2.0 * k2w + 2.0 * k3w + k4w);
+            }
         }
         g_ex = g_ex_next;
         dg_ex = dg_ex_next;
@@ -868,6 +889,12 @@ void oracle_set_exp_perturbation(oracle_sim* s, double rate) {
     if (!s) return;
     s->pe.exp_perturb = rate;
     s->pi.exp_perturb = rate;
+}
+
+void oracle_set_contraction(oracle_sim* s, int on) {
+    if (!s) return;
+    s->pe.contract = on != 0;
+    s->pi.contract = on != 0;
 }
 
 }  // extern "C"

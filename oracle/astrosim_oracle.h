@@ -89,6 +89,14 @@ double oracle_build_seconds(oracle_sim* s);
  */
 void oracle_set_exp_perturbation(oracle_sim* s, double rate);
 
+/*
+ * Sensitivity probe: from now on, evaluate the AdEx right-hand side and the
+ * neuron's RK4 stage arguments and update with fused multiply-adds (each product
+ * fused into the sum that consumes it, as a GPU compiler contracts them), a second
+ * correct rounding of the same formulas.  0 restores separate roundings.
+ */
+void oracle_set_contraction(oracle_sim* s, int on);
+
 #ifdef __cplusplus
 }
 #endif

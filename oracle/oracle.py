@@ -59,6 +59,7 @@ def lib():
         L.oracle_build_seconds.restype = C.c_double
         L.oracle_build_seconds.argtypes = [P]
         L.oracle_set_exp_perturbation.argtypes = [P, C.c_double]
+        L.oracle_set_contraction.argtypes = [P, C.c_int]
         _lib = L
     return _lib
 
@@ -127,6 +128,10 @@ class OracleSim:
     def perturb_exp(self, rate):
         """Moves the AdEx exponential one ulp for a fraction `rate` of its arguments (0: off)."""
         lib().oracle_set_exp_perturbation(self._h, float(rate))
+
+    def contract(self, on=True):
+        """Evaluates the neuron update with fused multiply-adds (a second correct rounding)."""
+        lib().oracle_set_contraction(self._h, 1 if on else 0)
 
     def step(self, n):
         lib().oracle_step(self._h, n)
