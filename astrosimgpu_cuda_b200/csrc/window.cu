@@ -149,6 +149,7 @@ Status window_setup(const RunConsts& rc, Network& net, bool fp32, WindowState& w
     AS_TRY(invert_csr(net.exc, net.own.n_lo, rc.n_exc, ws.fwd.exc_rs, ws.fwd.exc_dst, nullptr, st));
     AS_TRY(invert_csr(net.inh, net.own.n_lo, net.sz.n_inh, ws.fwd.inh_rs, ws.fwd.inh_dst, nullptr, st));
     AS_TRY(invert_csr(net.e2a, net.own.a_lo, rc.n_exc, ws.fwd.e2a_rs, ws.fwd.e2a_astro, &ws.fwd.e2a_pos, st));
+    AS_TRY(invert_csr(net.sic, net.own.n_lo, rc.n_astro, ws.fwd.sic_rs, ws.fwd.sic_dst, nullptr, st));
     // Windows with more spikes than this use the pull gather instead of deposits.
     // ASTROSIM_PUSH_LIMIT overrides it (the tests force the pull path with 0).
     ws.push_limit = static_cast<u32>(std::max<u64>(1024, nN / 50));
@@ -164,6 +165,7 @@ Status window_setup(const RunConsts& rc, Network& net, bool fp32, WindowState& w
     AS_TRY(ws.spk_count.alloc_zero(2, st));
     AS_TRY(ws.sic_win.alloc_zero(2 * nA * ws.W * rb, st));
     AS_TRY(ws.astro_active.alloc_zero(2 * ((nA + 31) / 32), st));
+    AS_TRY(ws.sic_flag.alloc_zero(2 * ((nN + 31) / 32), st));
     AS_TRY(ws.mode.alloc_zero(2, st));
     AS_CUDA(cudaStreamSynchronize(st));
     return Status::Ok();

@@ -13,7 +13,10 @@
 //   - pull (a busy window, or a target whose slots overflowed): the target walks its
 //     CSR rows against the previous window's per-neuron spike words, exactly like
 //     the per-step gather.
-// SIC factors are pulled through a per-window "astrocyte active" bitmask.
+// SIC factors are pulled through a per-window "astrocyte active" bitmask, by the
+// neurons that the push flagged: those whose a2n row holds an astrocyte that was
+// active (the push walks each active astrocyte's forward a2n list), so a window
+// without active astrocytes costs every other neuron one flag-word read.
 #pragma once
 
 #include "common.cuh"
@@ -37,6 +40,7 @@ struct ForwardCSR {
     DevBuf<u32> exc_rs, exc_dst;            // excitatory source -> neuron targets
     DevBuf<u32> inh_rs, inh_dst;            // stored inhibitory id -> neuron targets
     DevBuf<u32> e2a_rs, e2a_astro, e2a_pos; // excitatory source -> (astrocyte, position in its row)
+    DevBuf<u32> sic_rs, sic_dst;            // astrocyte -> neurons whose a2n rows hold it
     u32 max_fanout = 0;
 };
 
@@ -52,6 +56,7 @@ struct WindowState {
     DevBuf<u32> spk_count;                    // [2]
     DevBuf<unsigned char> sic_win;            // [2][n_astro][W] real
     DevBuf<u32> astro_active;                 // [2][ceil(n_astro / 32)]
+    DevBuf<u32> sic_flag;                     // [2][ceil(n_neurons / 32)]: a2n row holds an active astrocyte
     DevBuf<int> mode;                         // [2]: 0 push, 1 pull
     // autotuner: (block size, launch bounds) variant of window_kernel, an index into
     // its table; -1 while timing the candidates, -2 for the generic kernel (a block

@@ -17,9 +17,10 @@ struct WinPtrs {
     u32* spk_count;                  // [2]
     R* sic_win;                      // [2][n_astro][W]
     u32* astro_active;               // [2][astro_words]
+    u32* sic_flag;                   // [2][neuron_words]
     int* mode;                       // [2]
-    const u32 *fe_rs, *fe_dst, *fi_rs, *fi_dst, *fa_rs, *fa_astro, *fa_pos;
-    u32 cap, push_limit, astro_words;
+    const u32 *fe_rs, *fe_dst, *fi_rs, *fi_dst, *fa_rs, *fa_astro, *fa_pos, *fs_rs, *fs_dst;
+    u32 cap, push_limit, astro_words, neuron_words;
     int W;
 };
 
@@ -36,6 +37,7 @@ inline WinPtrs<R> win_ptrs(WindowState& ws, const RunConsts& rc) {
     w.spk_count = ws.spk_count.get();
     w.sic_win = reinterpret_cast<R*>(ws.sic_win.get());
     w.astro_active = ws.astro_active.get();
+    w.sic_flag = ws.sic_flag.get();
     w.mode = ws.mode.get();
     w.fe_rs = ws.fwd.exc_rs.get();
     w.fe_dst = ws.fwd.exc_dst.get();
@@ -44,9 +46,12 @@ inline WinPtrs<R> win_ptrs(WindowState& ws, const RunConsts& rc) {
     w.fa_rs = ws.fwd.e2a_rs.get();
     w.fa_astro = ws.fwd.e2a_astro.get();
     w.fa_pos = ws.fwd.e2a_pos.get();
+    w.fs_rs = ws.fwd.sic_rs.get();
+    w.fs_dst = ws.fwd.sic_dst.get();
     w.cap = ws.push_limit + 1;
     w.push_limit = ws.push_limit;
     w.astro_words = (rc.n_astro + 31) / 32;
+    w.neuron_words = (rc.n_neurons + 31) / 32;
     w.W = ws.W;
     return w;
 }
@@ -129,10 +134,15 @@ __device__ __forceinline__ void neuron_window(const RunConsts& rc, const NetScal
     }
     if (window_done && c) w.nin_cnt[slot_base] = 0;
 
-    // SIC factors of the previous window through the active-astrocyte bitmask
+    // SIC factors of the previous window through the active-astrocyte bitmask, for a
+    // neuron the push flagged (its a2n row holds an astrocyte that was active); for
+    // the others every factor in the row is 0, the same as the walk would find
     R sic_acc[kMaxWindow];
     bool sic_input = false;
-    {
+    u32* flag_word = w.sic_flag + static_cast<u64>(buf) * w.neuron_words + (j >> 5);
+    const u32 flag_bit = 1u << (j & 31);
+    if (*flag_word & flag_bit) {
+        if (window_done) atomicAnd(flag_word, ~flag_bit);  // clean for the window after next
         const u32* act = w.astro_active + static_cast<u64>(prev) * w.astro_words;
         const R* fac = w.sic_win + static_cast<u64>(prev) * ns.n_astro * W;
         const u32 k1 = p.sic_rs[j + 1];
@@ -296,9 +306,10 @@ __device__ __forceinline__ void window_cells(const RunConsts& rc, const NetScala
         neuron_window<R, false>(rc, ns, rc.pi, p, w, j, win_start, s_begin, s_end, buf, pull, window_done);
 }
 
-// After window `buf` completes: deliver its spikes into the inboxes of the next
+// After window `buf` completes: flag the neurons whose a2n rows hold an astrocyte
+// that was active in it, then deliver its spikes into the inboxes of the next
 // window (buffer buf ^ 1), or switch the next window to pull when it was busy.
-// Blocks 0 .. n_blk-1 share the spike list.
+// Blocks 0 .. n_blk-1 share the spike list and the active-astrocyte words.
 // Targets outside [t_lo, t_hi) (neurons) and [a_lo, a_hi) (astrocytes) are skipped:
 // a rank of a sharded network delivers only into the cells it owns.
 template <typename R>
@@ -312,10 +323,27 @@ __device__ __forceinline__ void push_cells(const WinPtrs<R>& w, u32 n_exc, u32 n
         w.mode[nxt] = busy ? 1 : 0;
         w.spk_count[nxt] = 0;  // the next window appends its spikes there
     }
-    if (busy) return;
     const u32 lane = threadIdx.x & 31;
     const u64 warp = (static_cast<u64>(blk) * blockDim.x + threadIdx.x) >> 5;
     const u64 n_warps = (static_cast<u64>(n_blk) * blockDim.x) >> 5;
+    {
+        // a warp per active astrocyte: flag its a2n targets for the next window
+        const u32* act = w.astro_active + static_cast<u64>(buf) * w.astro_words;
+        u32* flags = w.sic_flag + static_cast<u64>(nxt) * w.neuron_words;
+        for (u64 wd = warp; wd < w.astro_words; wd += n_warps) {
+            u32 bits = act[wd];
+            while (bits) {
+                const u32 a = static_cast<u32>(wd * 32) + static_cast<u32>(__ffs(bits) - 1);
+                bits &= bits - 1;
+                for (u32 k = w.fs_rs[a] + lane; k < w.fs_rs[a + 1]; k += 32) {
+                    const u32 t = w.fs_dst[k];
+                    if (t < t_lo || t >= t_hi) continue;
+                    atomicOr(&flags[t >> 5], 1u << (t & 31));
+                }
+            }
+        }
+    }
+    if (busy) return;
     const R* vals = w.spk_val + static_cast<u64>(buf) * w.W * n_neurons;
     for (u64 e = warp; e < n; e += n_warps) {
         const u32 packed = w.spk_list[static_cast<u64>(buf) * w.cap + e];

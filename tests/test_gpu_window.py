@@ -71,3 +71,34 @@ def test_every_launch_variant_is_bit_identical(monkeypatch, precision):
         for k in STATES + ("counts",):
             np.testing.assert_array_equal(got[k], ref[k], err_msg=f"{k} block {block} variant {v}")
     monkeypatch.delenv("ASTROSIM_WINDOW_VARIANT", raising=False)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_many_active_astrocytes_windowed_matches_per_step(monkeypatch, precision):
+    """A low SIC threshold makes most astrocytes active: the push flags the neurons
+    whose a2n rows hold an active astrocyte and only those walk their rows; results
+    equal the per-step path's, over irregular chunks (partial windows), push and pull."""
+    bio = {"SIC_th": 0.074, "w_a2n": 3.0}
+    kw = dict(n_total=6000, seed=13, pre_ms=10, sim_ms=90, precision=precision, raster_steps=1000)
+    chunks = (7, 3, 120, 451, 419)
+    monkeypatch.setenv("ASTROSIM_STEPPER", "plain")
+    with asg.Simulation(biology=bio, **kw) as s:
+        for c in chunks:
+            s.step(c)
+        ref = {k: s.state(k) for k in STATES}
+        ref["counts"] = s.spike_counts()
+        ref_active = int((s.state("sic_factor") > 0).sum())
+    for push_limit in (None, 0):
+        monkeypatch.setenv("ASTROSIM_STEPPER", "auto")
+        if push_limit is None:
+            monkeypatch.delenv("ASTROSIM_PUSH_LIMIT", raising=False)
+        else:
+            monkeypatch.setenv("ASTROSIM_PUSH_LIMIT", str(push_limit))
+        with asg.Simulation(biology=bio, **kw) as s:
+            for c in chunks:
+                s.step(c)
+            for k in STATES:
+                np.testing.assert_array_equal(s.state(k), ref[k], err_msg=f"{k} push_limit={push_limit}")
+            np.testing.assert_array_equal(s.spike_counts(), ref["counts"])
+    monkeypatch.delenv("ASTROSIM_PUSH_LIMIT", raising=False)
+    assert ref_active > 100, ref_active
