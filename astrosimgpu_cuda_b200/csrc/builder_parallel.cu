@@ -165,6 +165,56 @@ __device__ __forceinline__ u64 walk_pre(const Sec& s, u64 c, u32 self_post, V& v
     return c;
 }
 
+// The third-factor test at tape position t: u(t) < P_THIRD.
+__device__ __forceinline__ bool third_hit(const Sec& s, u64 t) {
+    return (rng_bits(s.seed, kSetupStream, t) >> 11) < kThirdLim;
+}
+
+// walk_pre for a walk that only needs the tape position it ends at, tuned for a
+// single long walk per thread: while a post's third-factor test resolves, the tests
+// of the next post at both positions it can take (one draw later if this test
+// misses, two if it hits and a pool pick follows) are hashed too, so each post
+// costs about the hashing throughput instead of a dependent hash latency.  It draws
+// the same positions in the same order and returns walk_pre's result.
+__device__ __forceinline__ u64 walk_pre_end(const Sec& s, u64 c, u32 self_post) {
+    u32 pos = 0;
+    const u32 n = s.post_count;
+    if (n == 0) return c;
+    u32 g = skip_at(s, c++);
+    if (!s.third) {
+        for (;;) {
+            if (g >= n - pos) break;
+            pos += g + 1;
+            if (pos >= n) break;
+            g = skip_at(s, c++);
+        }
+        return c;
+    }
+    bool hit_here = third_hit(s, c);  // c is the test position of the coming post
+    for (;;) {
+        if (g >= n - pos) break;  // the skip reaches the end of the block
+        pos += g;
+        const u32 post = s.post_off + pos;
+        ++pos;
+        const bool more = pos < n;
+        if (post == self_post) {  // autapse: no draws; the next skip is at c
+            if (!more) break;
+            g = skip_at(s, c++);
+            hit_here = third_hit(s, c);
+            continue;
+        }
+        const u32 g_miss = skip_peek(s, c + 1), g_hit = skip_peek(s, c + 2);
+        const bool next_miss = third_hit(s, c + 2), next_hit = third_hit(s, c + 3);
+        const bool hit = hit_here;
+        c += hit ? 2 : 1;  // the test, and the pool pick after a hit
+        if (!more) break;
+        g = skip_checked(s, c, hit ? g_hit : g_miss);
+        ++c;
+        hit_here = hit ? next_hit : next_miss;
+    }
+    return c;
+}
+
 // ---------------------------------------------------------------- pools
 __global__ void pool_pass_kernel(u64 seed, u32 n_neurons, u32 n_astro, u32 take, u64 base, const u64* prefix,
                                  u32* pool, u64* extra) {
@@ -395,9 +445,8 @@ __global__ void remerge_kernel(Sec s, const Hazard* hz, u32 n_hz, const u64* orb
     u64 c = orbit[hz[h].r];
     u64* mine = expl + static_cast<u64>(h) * max_explicit;
     mine[out.m++] = c;
-    NoVisit nv;
     for (;;) {
-        c = walk_pre(s, c, static_cast<u32>(r), nv);
+        c = walk_pre_end(s, c, static_cast<u32>(r));
         ++r;
         if (r >= static_cast<long long>(n_pres)) {
             out.end = c;
