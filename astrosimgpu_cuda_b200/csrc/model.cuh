@@ -380,7 +380,6 @@ __device__ __forceinline__ void astro_rhs(const AstroK& c, double Ca_tot, double
     dIP3 = div_by(IP3_0 - IP3, tau_IP3, rcp_tau_IP3);
     dh = alpha_h * (1.0 - h) - beta_h * h;
 }
-#endif
 
 __device__ __forceinline__ double exp_r(double x) { return exp(x); }
 __device__ __forceinline__ float exp_r(float x) { return expf(x); }
@@ -460,6 +459,8 @@ __device__ __forceinline__ void astro_rhs_fast(const AstroK& c, float Ca_tot, fl
     dh = alpha_h * (1.0f - h) - beta_h * h;
 }
 
+#endif  // __CUDACC__ (the right-hand sides are device code)
+
 // A run constant in the stage type: the double value, or its float copy.
 template <typename R>
 __host__ __device__ __forceinline__ R as_r(double d, float f);
@@ -468,6 +469,7 @@ __host__ __device__ __forceinline__ double as_r<double>(double d, float) { retur
 template <>
 __host__ __device__ __forceinline__ float as_r<float>(double, float f) { return f; }
 
+#ifdef __CUDACC__
 // Box-Muller in float from one stream (counters 0 and 1): the noise draws of the FP32 form.
 __device__ __forceinline__ float normal_fast(u64 base) {
 #ifdef ASTROSIM_FP32_IEEE
@@ -485,5 +487,7 @@ __device__ __forceinline__ float normal_fast(u64 base) {
     return sqrt_ftz(-2.0f * log_fast(u1)) * cos_ftz(static_cast<float>(kTwoPi) * u2);
 #endif
 }
+
+#endif  // __CUDACC__
 
 }  // namespace astrosim
