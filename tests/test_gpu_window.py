@@ -74,11 +74,14 @@ def test_every_launch_variant_is_bit_identical(monkeypatch, precision):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_many_active_astrocytes_windowed_matches_per_step(monkeypatch, precision):
-    """A low SIC threshold makes most astrocytes active: the push flags the neurons
-    whose a2n rows hold an active astrocyte and only those walk their rows; results
-    equal the per-step path's, over irregular chunks (partial windows), push and pull."""
-    bio = {"SIC_th": 0.074, "w_a2n": 3.0}
+@pytest.mark.parametrize("sic_th,w_a2n,min_active", [(0.06, 3.0, 1000), (0.0705, 1.0, 100), (0.071, 1.0, 10)])
+def test_active_astrocytes_windowed_matches_per_step(monkeypatch, precision, sic_th, w_a2n, min_active):
+    """Lowered SIC thresholds make every astrocyte, a few hundred or a few tens of
+    them active (the oracle at these settings: 1200, 140-310 and 16-48 of 1200
+    active from 20 ms on).  The push flags the neurons whose a2n rows hold an active
+    astrocyte and only those walk their rows; results equal the per-step path's,
+    over irregular chunks (partial windows), with push and with pull delivery."""
+    bio = {"SIC_th": sic_th, "w_a2n": w_a2n}
     kw = dict(n_total=6000, seed=13, pre_ms=10, sim_ms=90, precision=precision, raster_steps=1000)
     chunks = (7, 3, 120, 451, 419)
     monkeypatch.setenv("ASTROSIM_STEPPER", "plain")
@@ -101,4 +104,4 @@ def test_many_active_astrocytes_windowed_matches_per_step(monkeypatch, precision
                 np.testing.assert_array_equal(s.state(k), ref[k], err_msg=f"{k} push_limit={push_limit}")
             np.testing.assert_array_equal(s.spike_counts(), ref["counts"])
     monkeypatch.delenv("ASTROSIM_PUSH_LIMIT", raising=False)
-    assert ref_active > 100, ref_active
+    assert ref_active >= min_active, ref_active
