@@ -37,15 +37,17 @@ DT = 0.1
 PRE_MS, SIM_MS = 100.0, 500.0
 
 
-# DRAM bytes (read + write) of one window_kernel launch measured by ncu
-# (profiles/): FP32 on the full N_total = 1e7 workload in the timed region (one
-# pass, nothing replayed), FP64 on the N_total = 1e6 steady state; traffic grows
-# with the cell count, so a launch at N carries about N / N_measured times this.
-PROFILED_WINDOW_TRAFFIC = {"fp32": (10_000_000, 2.016e9, "ncu at N_total=1e7, timed region"),
-                           "fp64": (1_000_000, 409.9e6, "ncu at N_total=1e6 steady state, scaled")}
-# Fraction of issue slots busy in the same captures: the window kernel is bound by
-# instruction issue, not by HBM, which is why roofline.frac against HBM stays low.
-PROFILED_ISSUE_ACTIVE = {"fp32": 0.728, "fp64": 0.559}
+# One steady-state window_kernel launch measured by ncu (profiles/), at
+# N_total = 3e6, where the state streamed per launch is several times the L2:
+# DRAM bytes read + written, warp instructions issued and the fraction of issue
+# slots busy.  Bytes and instructions grow with the cell count, so a launch at N
+# carries about N / 3e6 times these.
+PROFILED_WINDOW = {
+    "fp32": {"n": 3_000_000, "dram": None, "warp_inst": None, "issue_busy": None},
+    "fp64": {"n": 3_000_000, "dram": None, "warp_inst": None, "issue_busy": None},
+}
+PROFILED_SOURCE = "ncu, one steady-state window_kernel launch at N_total=3e6 (profiles/), scaled to N_total"
+SCHEDULERS_PER_SM = 4  # warp schedulers per B200 SM: one warp instruction each per cycle at most
 
 
 def peaks():
@@ -161,22 +163,61 @@ def window_step_bytes(s, precision, spikes_per_step, window=10):
     """Algorithmic bytes per time step of the windowed engine (one launch per window).
 
     Per window each neuron reads V, w, V_reset, b (32 B), five conductance/SIC
-    values, its refractory counter and inbox count (8 B) and its a2n row (8 B of
-    row_start + 4 B per astrocyte source), and writes V, w, the five values, the
-    counter and its spike word; each astrocyte reads Ca, IP3, h, four parameters,
-    its inbox count and flag, and writes Ca, IP3, h, `window` SIC factors, its flag
-    and last factor.  Each spike delivers one deposit (key, step, value: 12 B FP32 /
-    16 B FP64, plus a 4 B count update) per outgoing edge.
+    values, its refractory counter and inbox count (8 B) and its a2n flag bit, and
+    writes V, w, the five values, the counter and its spike word; a neuron whose a2n
+    row holds an active astrocyte also reads the row (8 B of row_start + 4 B per
+    entry; estimated from the active astrocytes at the last step times their a2n
+    fan-out).  Each astrocyte reads Ca, IP3, h, four parameters, its inbox count and
+    flag, and writes Ca, IP3, h, `window` SIC factors, its flag and last factor.
+    Each spike delivers one deposit (key, step, value: 12 B FP32 / 16 B FP64, plus a
+    4 B count update) per outgoing edge.
     """
     r = 8 if precision == "fp64" else 4
     nn = s["n_exc"] + s["n_inh"]
     na = s["n_astro"]
-    sic_ids = 4 * s["n_sic_edges"]
-    neuron = nn * (32 + 5 * r + 8 + 8 + 16 + 5 * r + 8) + sic_ids
+    a2n_fanout = s["n_sic_edges"] / max(1, na)
+    flagged = min(nn, s.get("active_astro", 0) * a2n_fanout)
+    row = s["n_sic_edges"] / max(1, nn)
+    neuron = nn * (32 + 5 * r + 8 + 1 / 8 + 16 + 5 * r + 8) + flagged * (8 + 4 * row)
     astro = na * (16 + r + 32 + 5 + 16 + r + window * r + 1 + r)
     fanout = (s["n_exc_edges"] + s["n_inh_edges"] + s["n_e2a_edges"]) / max(1, nn)
     deposits = spikes_per_step * window * fanout * ((16 if r == 8 else 12) + 4)
     return (neuron + astro + deposits) / window
+
+
+def sm_count(device):
+    try:
+        import torch
+        return torch.cuda.get_device_properties(device).multi_processor_count
+    except Exception:
+        return 148
+
+
+def roofline(leg, prec, achieved, peak, peak_kind, ms_step, device):
+    """The window kernel's roofline: HBM bytes against the measured copy bandwidth,
+    and, since the kernel is bound by instruction issue, warp instructions issued
+    against one per scheduler per cycle at the SM clock sampled during the run."""
+    prof = PROFILED_WINDOW[prec]
+    scale = N_TOTAL / prof["n"]
+    out = {"bound": "issue", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+           "traffic": prof["dram"] * scale if prof["dram"] else None,
+           "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum, " + PROFILED_SOURCE,
+           "peak_source": peak_kind,
+           "kernel": f"window_kernel<{'float' if prec == 'fp32' else 'double'}> (one launch = one 10-step window, "
+                     f"its push_kernel inside the timed duration)",
+           "algorithmic_bytes_per_step": leg["bytes"],
+           "gather_formulation_bytes_per_step": leg["gather_bytes"],
+           "gather_formulation_equivalent_gbs": leg["gather_bytes"] / (ms_step * 1e-3) / 1e9}
+    mhz = (leg.get("clocks") or {}).get("sm_mhz")
+    if prof["warp_inst"] and mhz:
+        inst_per_step = prof["warp_inst"] * scale / 10
+        achieved_ips = inst_per_step / (ms_step * 1e-3)
+        peak_ips = sm_count(device) * SCHEDULERS_PER_SM * mhz * 1e6
+        out["issue"] = {"achieved_warp_inst_per_s": achieved_ips, "peak_warp_inst_per_s": peak_ips,
+                        "frac": achieved_ips / peak_ips, "sm_mhz": mhz,
+                        "warp_inst_per_step": inst_per_step,
+                        "issue_slots_busy_ncu": prof["issue_busy"], "source": PROFILED_SOURCE}
+    return out
 
 
 def timed_launches(first, n, window=10):
@@ -616,22 +657,7 @@ def main():
         "syn_events_definition": "edge visits of the reference's per-step gather formulation (every CSR entry "
                                  "once per step: E_visit x steps/s); the windowed push engine reads only the "
                                  "edges of sources that spiked, so this is equivalent work, not work done",
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": PROFILED_WINDOW_TRAFFIC["fp32" if "fp32" in res else "fp64"][1] * N_TOTAL /
-                                PROFILED_WINDOW_TRAFFIC["fp32" if "fp32" in res else "fp64"][0],
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one window_kernel launch, "
-                                       + PROFILED_WINDOW_TRAFFIC["fp32" if "fp32" in res else "fp64"][2]
-                                       + " (profiles/)",
-                     "peak_source": peak_kind,
-                     "issue_slots_busy": PROFILED_ISSUE_ACTIVE["fp32" if "fp32" in res else "fp64"],
-                     "issue_source": "ncu smsp__issue_active of the same window_kernel capture (profiles/)",
-                     "kernel": "window_kernel<float> (one launch = one 10-step window); its push_kernel, 1.5 % of "
-                               "the window time in the launch list, is inside the timed duration",
-                     "algorithmic_bytes_per_launch": f32["bytes"] * 10,
-                     "launch_ms": ms_step * 10,
-                     "algorithmic_bytes_per_step": f32["bytes"],
-                     "gather_formulation_bytes_per_step": f32["gather_bytes"],
-                     "gather_formulation_equivalent_gbs": f32["gather_bytes"] / (ms_step * 1e-3) / 1e9},
+        "roofline": roofline(f32, "fp32" if "fp32" in res else "fp64", achieved, peak, peak_kind, ms_step, local),
         "spikes_per_step": f32["spikes_per_step"],
         "e2e": extra["e2e"],
         "gpu_launches": timed_launches(f32["summary"]["steps_done"] - args.steps, args.steps) +
