@@ -200,6 +200,33 @@ __device__ __forceinline__ void astro_cell_step(const RunConsts& rc, const NetSc
     p.sic_last[a] = factor;
 }
 
+// The AdEx right-hand side at one set of conductances (each RK4 step uses three:
+// the step's start, its midpoint and its end).  FP64: the reference's term-by-term
+// formula (neuron_rhs, src/astrosim_fused.cu:281-290).  FP32 form: the refolded
+// formula (adex_rhs_folded), its conductance terms computed once per set.
+template <typename R>
+struct AdexStage {
+    const NeuronK& p;
+    R g_ex, g_in, I_ext;
+    __device__ __forceinline__ AdexStage(const NeuronK& pk, R gex, R gin, R iext)
+        : p(pk), g_ex(gex), g_in(gin), I_ext(iext) {}
+    __device__ __forceinline__ void operator()(R V, R w, R& dV, R& dw) const {
+        neuron_rhs(p, V, w, g_ex, g_in, I_ext, dV, dw);
+    }
+};
+#ifndef ASTROSIM_FP32_IEEE
+template <>
+struct AdexStage<float> {
+    const NeuronK& p;
+    AdexCoef c;
+    __device__ __forceinline__ AdexStage(const NeuronK& pk, float gex, float gin, float iext)
+        : p(pk), c(adex_coef(pk, gex, gin, fmaf(iext, pk.f_inv_Cm, pk.f_C0))) {}
+    __device__ __forceinline__ void operator()(float V, float w, float& dV, float& dw) const {
+        adex_rhs_folded(p, c, V, w, dV, dw);
+    }
+};
+#endif
+
 // Register-resident state of one neuron.
 template <typename R>
 struct NeuronRegs {
@@ -248,19 +275,21 @@ __device__ __forceinline__ bool neuron_advance_step(const RunConsts& rc, const N
         if (refractory > 0) {
             V = n.V_reset;
             R dV, dw;
-            neuron_rhs(pk, static_cast<R>(V), static_cast<R>(w), g_ex, g_in, I_ext, dV, dw);
+            const AdexStage<R> r0(pk, g_ex, g_in, I_ext);
+            r0(static_cast<R>(V), static_cast<R>(w), dV, dw);
             w += static_cast<double>(hs * dw);
         } else {
             const R g_ex_mid = static_cast<R>(0.5) * (g_ex + g_ex_next);
             const R g_in_mid = static_cast<R>(0.5) * (g_in + g_in_next);
             const R v = static_cast<R>(V), ww = static_cast<R>(w);
             R k1V, k1w, k2V, k2w, k3V, k3w, k4V, k4w;
-            neuron_rhs(pk, v, ww, g_ex, g_in, I_ext, k1V, k1w);
-            neuron_rhs(pk, v + static_cast<R>(0.5) * hs * k1V, ww + static_cast<R>(0.5) * hs * k1w, g_ex_mid,
-                          g_in_mid, I_ext, k2V, k2w);
-            neuron_rhs(pk, v + static_cast<R>(0.5) * hs * k2V, ww + static_cast<R>(0.5) * hs * k2w, g_ex_mid,
-                          g_in_mid, I_ext, k3V, k3w);
-            neuron_rhs(pk, v + hs * k3V, ww + hs * k3w, g_ex_next, g_in_next, I_ext, k4V, k4w);
+            const AdexStage<R> r1(pk, g_ex, g_in, I_ext);
+            r1(v, ww, k1V, k1w);
+            const AdexStage<R> rm(pk, g_ex_mid, g_in_mid, I_ext);
+            rm(v + static_cast<R>(0.5) * hs * k1V, ww + static_cast<R>(0.5) * hs * k1w, k2V, k2w);
+            rm(v + static_cast<R>(0.5) * hs * k2V, ww + static_cast<R>(0.5) * hs * k2w, k3V, k3w);
+            const AdexStage<R> r4(pk, g_ex_next, g_in_next, I_ext);
+            r4(v + hs * k3V, ww + hs * k3w, k4V, k4w);
             V += static_cast<double>(h6 * (k1V + static_cast<R>(2.0) * k2V + static_cast<R>(2.0) * k3V + k4V));
             w += static_cast<double>(h6 * (k1w + static_cast<R>(2.0) * k2w + static_cast<R>(2.0) * k3w + k4w));
         }
