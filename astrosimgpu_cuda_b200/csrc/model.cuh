@@ -186,12 +186,14 @@ struct AstroK {
     double SIC_scale, SIC_th;
     // Folded constants of the FP32 form (its stages multiply by reciprocals).
     float f_inv_ratio, f_ratio_rate_IP3R, f_ratio_rate_L, f_k_Kd_inh, f_Km2;
+    // 1 + 1 / ratio_ER_cyt and rate_SERCA * Km_SERCA^2, for the refolded FP32 form.
+    float f_1p_inv_ratio, f_rate_Km2;
     // Float copies read by the FP32 stages (converted once here, not per use).
     float f_Kd_IP3_1, f_Kd_IP3_2, f_Kd_act, f_rate_SERCA, f_k_IP3R, f_SIC_scale;
-    float pad_;        // explicit, zero: the struct has no implicit padding
+    float pad_[3];     // explicit, zero: the struct has no implicit padding
     double rcp_ratio;  // RN(1 / ratio_ER_cyt), for the exact division by a constant (div_by)
 };
-static_assert(sizeof(AstroK) == 12 * 8 + 12 * 4 + 8, "AstroK has no implicit padding");
+static_assert(sizeof(AstroK) == 12 * 8 + 16 * 4 + 8, "AstroK has no implicit padding");
 
 // AdEx neuron constants for one population (src/astrosim_fused.cu:228-232).
 struct NeuronK {
@@ -266,6 +268,8 @@ inline AstroK astro_constants(const Biology& b) {  // src/astrosim_fused.cu:935-
     k.f_ratio_rate_L = static_cast<float>(b.ratio_ER_cyt * b.rate_L);
     k.f_k_Kd_inh = static_cast<float>(b.k_IP3R * b.Kd_inh);
     k.f_Km2 = static_cast<float>(b.Km_SERCA * b.Km_SERCA);
+    k.f_1p_inv_ratio = static_cast<float>(1.0 + 1.0 / b.ratio_ER_cyt);
+    k.f_rate_Km2 = static_cast<float>(b.rate_SERCA * b.Km_SERCA * b.Km_SERCA);
     k.f_Kd_IP3_1 = static_cast<float>(b.Kd_IP3_1);
     k.f_Kd_IP3_2 = static_cast<float>(b.Kd_IP3_2);
     k.f_Kd_act = static_cast<float>(b.Kd_act);
@@ -493,32 +497,40 @@ __device__ __forceinline__ void astro_rhs_fast(const AstroK& c, float Ca_tot, fl
                                                float Ca, float IP3, float h, float noise, float& dCa, float& dIP3,
                                                float& dh) {
 #ifdef ASTROSIM_FP32_IEEE
+    // the FP64 formula's operations in float (the measurement build)
     const float Ca_ER = (Ca_tot - Ca) / static_cast<float>(c.ratio_ER_cyt);
-#else
-    const float Ca_ER = (Ca_tot - Ca) * c.f_inv_ratio;
-#endif
     const float m_inf = div_fast(IP3, IP3 + c.f_Kd_IP3_1);
     const float n_inf = div_fast(Ca, Ca + c.f_Kd_act);
     const float m3 = m_inf * m_inf * m_inf;
     const float n3 = n_inf * n_inf * n_inf;
     const float h3 = h * h * h;
-#ifdef ASTROSIM_FP32_IEEE
     const float J_channel =
         static_cast<float>(c.ratio_ER_cyt) * static_cast<float>(c.rate_IP3R) * m3 * n3 * h3 * (Ca_ER - Ca);
-#else
-    const float J_channel = c.f_ratio_rate_IP3R * m3 * n3 * h3 * (Ca_ER - Ca);
-#endif
     const float J_pump = div_fast(c.f_rate_SERCA * Ca * Ca, c.f_Km2 + Ca * Ca);
     const float J_leak = c.f_ratio_rate_L * (Ca_ER - Ca);
     const float alpha_h = div_fast(c.f_k_Kd_inh * (IP3 + c.f_Kd_IP3_1), IP3 + c.f_Kd_IP3_2);
     const float beta_h = c.f_k_IP3R * Ca;
     dCa = J_channel - J_pump + J_leak + noise;
-#ifdef ASTROSIM_FP32_IEEE
     dIP3 = (IP3_0 - IP3) / tau_IP3;
-#else
-    dIP3 = (IP3_0 - IP3) * inv_tau_IP3;
-#endif
     dh = alpha_h * (1.0f - h) - beta_h * h;
+    (void)inv_tau_IP3;
+#else
+    // Refolded (the same formula, fewer roundings and operations): with d = Ca_ER - Ca,
+    // J_channel + J_leak = d (ratio rate_IP3R (m_inf n_inf)^3 h^3 + ratio rate_L),
+    // m_inf n_inf = IP3 Ca / ((IP3 + Kd_IP3_1)(Ca + Kd_act)) with one reciprocal, and
+    // J_pump = rate_SERCA - rate_SERCA Km^2 / (Km^2 + Ca^2).
+    const float d = fmaf(-Ca, c.f_1p_inv_ratio, Ca_tot * c.f_inv_ratio);
+    const float ip_k1 = IP3 + c.f_Kd_IP3_1;
+    const float mn = (IP3 * Ca) * rcp_ftz(ip_k1 * (Ca + c.f_Kd_act));
+    const float mn3 = mn * mn * mn;
+    const float h3 = h * h * h;
+    const float J_pump = fmaf(-c.f_rate_Km2, rcp_ftz(fmaf(Ca, Ca, c.f_Km2)), c.f_rate_SERCA);
+    dCa = fmaf(d, fmaf(c.f_ratio_rate_IP3R * mn3, h3, c.f_ratio_rate_L), noise - J_pump);
+    const float alpha_h = (c.f_k_Kd_inh * ip_k1) * rcp_ftz(IP3 + c.f_Kd_IP3_2);
+    dIP3 = fmaf(-IP3, inv_tau_IP3, IP3_0 * inv_tau_IP3);
+    dh = fmaf(-h, fmaf(c.f_k_IP3R, Ca, alpha_h), alpha_h);
+    (void)tau_IP3;
+#endif
 }
 
 #endif  // __CUDACC__ (the right-hand sides are device code)
