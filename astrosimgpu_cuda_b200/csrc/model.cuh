@@ -122,29 +122,6 @@ __host__ __device__ __forceinline__ int rng_poisson_at(u64 base, double lambda, 
     return count;
 }
 
-// rng_poisson_at with the stream's first draw already hashed: m0 = rng_mix(base) >> 11
-// (callers hash it ahead, one step early, so its latency overlaps other work).
-__host__ __device__ __forceinline__ int rng_poisson_from(u64 base, u64 m0, double lambda, double limit, u64 lim53) {
-    if (lambda <= 0.0) return 0;
-    if (lambda > 30.0) {
-        double u1 = static_cast<double>(m0) * (1.0 / 9007199254740992.0);
-        if (u1 <= 1e-300) u1 = 1e-300;
-        const double u2 = rng_uniform_at(base, 1);
-        const double z = sqrt(-2.0 * log(u1)) * cos(kTwoPi * u2);
-        const double v = lambda + sqrt(lambda) * z;
-        return v < 0.0 ? 0 : static_cast<int>(v + 0.5);
-    }
-    if (m0 <= lim53) return 0;
-    double product = static_cast<double>(m0) * (1.0 / 9007199254740992.0);
-    int count = 0;
-    u64 c = 1;
-    do {
-        ++count;
-        product *= rng_uniform_at(base, c++);
-    } while (product > limit);
-    return count;
-}
-
 // Stream-selection constants of the per-step draws (src/astrosim_fused.cu:395, 404, 476, 499).
 constexpr u64 kAstroPoissonKey = 0xC2B2AE3D27D4EB4FULL;
 constexpr u64 kAstroNoiseKey = 0x9E3779B97F4A7C15ULL;
@@ -544,27 +521,22 @@ template <>
 __host__ __device__ __forceinline__ float as_r<float>(double, float f) { return f; }
 
 #ifdef __CUDACC__
-// Box-Muller in float from the hashed counters 0 and 1 of one stream
-// (h0 = rng_mix(base), h1 = rng_mix(base + kCounterMul)): the noise draws of the FP32 form.
-__device__ __forceinline__ float normal_fast_from(u64 h0, u64 h1) {
+// Box-Muller in float from one stream (counters 0 and 1): the noise draws of the FP32 form.
+__device__ __forceinline__ float normal_fast(u64 base) {
 #ifdef ASTROSIM_FP32_IEEE
     // the FP64 path's 53-bit uniforms, rounded to float; its u1 <= 1e-300 clamp
     // (src/astrosim_fused.cu:146) becomes log(1e-300) for an all-zero draw
-    const double d1 = static_cast<double>(h0 >> 11) * (1.0 / 9007199254740992.0);
-    const double d2 = static_cast<double>(h1 >> 11) * (1.0 / 9007199254740992.0);
+    const double d1 = rng_uniform_at(base, 0);
+    const double d2 = rng_uniform_at(base, 1);
     const float l1 = d1 > 0.0 ? log_fast(static_cast<float>(d1)) : -690.775528f;
     return sqrt_ftz(-2.0f * l1) * cos_ftz(static_cast<float>(kTwoPi) * static_cast<float>(d2));
 #else
-    const u32 a = static_cast<u32>(h0 >> 40);
-    const u32 b = static_cast<u32>(h1 >> 40);
+    const u32 a = static_cast<u32>(rng_mix(base) >> 40);
+    const u32 b = static_cast<u32>(rng_mix(base + kCounterMul) >> 40);
     const float u1 = (static_cast<float>(a) + 0.5f) * (1.0f / 16777216.0f);
     const float u2 = static_cast<float>(b) * (1.0f / 16777216.0f);
     return sqrt_ftz(-2.0f * log_fast(u1)) * cos_ftz(static_cast<float>(kTwoPi) * u2);
 #endif
-}
-
-__device__ __forceinline__ float normal_fast(u64 base) {
-    return normal_fast_from(rng_mix(base), rng_mix(base + kCounterMul));
 }
 
 #endif  // __CUDACC__

@@ -125,42 +125,27 @@ __device__ __forceinline__ void astro_advance(const AstroK& c, AstroRegs<R>& s, 
     }
 }
 
-// The hashed draws an astrocyte step starts from: the Poisson stream's first draw
-// and the noise stream's counters 0 and 1 (rng_mix of each), hashed ahead of the
-// step so that their latency overlaps the step before.
-struct AstroDraws {
-    u64 p0, n0, n1;
-};
-__device__ __forceinline__ AstroDraws astro_draws(u64 poisson_base, u64 noise_base) {
-    return AstroDraws{rng_mix(poisson_base), rng_mix(noise_base), rng_mix(noise_base + kCounterMul)};
-}
-
 // Everything astrocyte `a` does in step `step` once its delayed spike sum is known
 // (src/astrosim_fused.cu:390-417): Poisson IP3 drive, noise, RK4, SIC factor.
-// `dr` holds the hashed first draws of poisson_base and noise_base.
 template <typename R>
 __device__ __forceinline__ R astro_advance_step(const RunConsts& rc, const NetScalars& ns, AstroRegs<R>& s, R gathered, u32 a, i64 step,
-                                                u64 poisson_base, u64 noise_base, const AstroDraws& dr) {
+                                                u64 poisson_base, u64 noise_base) {
     R ip3_input = as_r<R>(rc.w_n2a, rc.f_w_n2a) * gathered;
     if (ns.lambda_astro > 0.0) {
-        const int ev = rng_poisson_from(poisson_base, dr.p0 >> 11, ns.lambda_astro, ns.limit_astro, ns.lim53_astro);
+        const int ev = rng_poisson_at(poisson_base, ns.lambda_astro, ns.limit_astro, ns.lim53_astro);
         if (ev > 0) ip3_input += as_r<R>(rc.weight_astro, rc.f_weight_astro) * static_cast<R>(ev);
     }
     R noise = static_cast<R>(0.0);
     if (rc.noise_astro > 0.0) {
-        u64 h0 = dr.n0, h1 = dr.n1;
-        if (!rc.independent_noise) {  // one noise stream per noise interval, shared by all astrocytes
-            const u64 base = rng_base(ns.seed ^ kAstroNoiseKey, static_cast<u64>(step / rc.steps_per_noise));
-            h0 = rng_mix(base);
-            h1 = rng_mix(base + kCounterMul);
-        }
+        u64 base = noise_base;
+        if (!rc.independent_noise)
+            base = rng_base(ns.seed ^ kAstroNoiseKey, static_cast<u64>(step / rc.steps_per_noise));
         if constexpr (std::is_same<R, float>::value) {
-            noise = rc.f_noise_astro * normal_fast_from(h0, h1);
+            noise = rc.f_noise_astro * normal_fast(base);
         } else {
-            // rng_normal (src/astrosim_fused.cu:143-149)
-            double u1 = static_cast<double>(h0 >> 11) * (1.0 / 9007199254740992.0);
+            double u1 = rng_uniform_at(base, 0);  // rng_normal (src/astrosim_fused.cu:143-149)
             if (u1 <= 1e-300) u1 = 1e-300;
-            const double u2 = static_cast<double>(h1 >> 11) * (1.0 / 9007199254740992.0);
+            const double u2 = rng_uniform_at(base, 1);
             noise = rc.noise_astro * (sqrt(-2.0 * log(u1)) * cos(kTwoPi * u2));
         }
     }
@@ -189,8 +174,8 @@ __device__ __forceinline__ void astro_cell_step(const RunConsts& rc, const NetSc
     const R gathered = gather_spikes<R>(p.e2a_rs, p.e2a_src, a, p.bits + static_cast<u64>(read_slot) * ns.words,
                                         p.val + static_cast<u64>(read_slot) * ns.n_neurons);
     AstroRegs<R> s = load_astro<R>(p.Ca[a], p.IP3[a], p.h[a], p.Ca_tot[a], p.IP3_0[a], p.tau_IP3[a], p.delta_IP3[a]);
-    const u64 pb = step_base(ns.seed, kAstroPoissonKey, step, a), nb = step_base(ns.seed, kAstroNoiseKey, step, a);
-    const R factor = astro_advance_step<R>(rc, ns, s, gathered, a, step, pb, nb, astro_draws(pb, nb));
+    const R factor = astro_advance_step<R>(rc, ns, s, gathered, a, step, step_base(ns.seed, kAstroPoissonKey, step, a),
+                                           step_base(ns.seed, kAstroNoiseKey, step, a));
     p.Ca[a] = s.Ca;
     p.IP3[a] = s.IP3;
     p.h[a] = s.h;
@@ -238,20 +223,19 @@ struct NeuronRegs {
 // Everything neuron j does in step `step` once its delayed sums are known
 // (src/astrosim_fused.cu:465-558): synaptic inputs, Poisson drive, SIC refresh,
 // noise, the alpha-cascade closed form and AdEx RK4 (or the refractory Euler step),
-// the spike test.  `noise` is noise_std * N(0,1) for this step when `has_noise`;
-// `poisson_m0` is rng_mix(poisson_base) >> 11, the Poisson stream's first draw.
+// the spike test.  `noise` is noise_std * N(0,1) for this step when `has_noise`.
 template <typename R>
 __device__ __forceinline__ bool neuron_advance_step(const RunConsts& rc, const NetScalars& ns, const NeuronK& pk,
                                                     bool excitatory,
                                                     NeuronRegs<R>& n, R exc_sum, R inh_sum, bool sic_refresh,
                                                     R sic_sum, bool has_noise, double noise, u64 poisson_base,
-                                                    u64 poisson_m0, R ex_decay, R in_decay) {
+                                                    R ex_decay, R in_decay) {
     R exc_input = as_r<R>(rc.w_e, rc.f_w_e) * exc_sum;
     const R inh_input = as_r<R>(-rc.w_i, rc.f_neg_w_i) * inh_sum;
     const double lambda = excitatory ? ns.lambda_exc : ns.lambda_inh;
     if (lambda > 0.0) {
-        const int ev = rng_poisson_from(poisson_base, poisson_m0, lambda, excitatory ? ns.limit_exc : ns.limit_inh,
-                                        excitatory ? ns.lim53_exc : ns.lim53_inh);
+        const int ev = rng_poisson_at(poisson_base, lambda, excitatory ? ns.limit_exc : ns.limit_inh,
+                                      excitatory ? ns.lim53_exc : ns.lim53_inh);
         if (ev > 0)
             exc_input += (excitatory ? as_r<R>(rc.weight_exc, rc.f_weight_exc) : as_r<R>(rc.weight_inh, rc.f_weight_inh)) *
                          static_cast<R>(ev);
@@ -379,9 +363,9 @@ __device__ __forceinline__ bool neuron_cell_step(const RunConsts& rc, const NetS
     const R hs = as_r<R>(rc.h_step, rc.f_h_step);
     const R ex_decay = exp_r(-hs / static_cast<R>(pk.tau_syn_ex));
     const R in_decay = exp_r(-hs / static_cast<R>(pk.tau_syn_in));
-    const u64 pbase = step_base(ns.seed, kNeuronPoissonKey, step, j);
     const bool spiked = neuron_advance_step<R>(rc, ns, pk, excitatory, n, exc_sum, inh_sum, sic_refresh, sic_sum,
-                                               has_noise, noise, pbase, rng_mix(pbase) >> 11, ex_decay, in_decay);
+                                               has_noise, noise, step_base(ns.seed, kNeuronPoissonKey, step, j),
+                                               ex_decay, in_decay);
     p.V[j] = n.V;
     p.w[j] = n.w;
     p.g_ex[j] = n.g_ex;

@@ -177,9 +177,6 @@ __device__ __forceinline__ void neuron_window(const RunConsts& rc, const NetScal
     double noise = 0.0;
     if (has_noise) noise = neuron_noise<R>(ns, nstd, nidx, j);
     u64 pbase = step_base(ns.seed, kNeuronPoissonKey, t0, j);
-    // the Poisson stream's first draw is hashed one step ahead, so that its latency
-    // overlaps the RK4 of the step before (the same values, in the same order)
-    u64 m0 = rng_mix(pbase) >> 11;
     u32 word = 0;
     R* vout = w.spk_val + static_cast<u64>(buf) * W * nN;
     for (int st = s_begin; st < s_end; ++st) {
@@ -187,13 +184,10 @@ __device__ __forceinline__ void neuron_window(const RunConsts& rc, const NetScal
         const bool refresh = since >= 0 && phase == 0;
         if (has_noise && nphase == 0 && st != s_begin) noise = neuron_noise<R>(ns, nstd, nidx, j);
         const R zero = static_cast<R>(0.0);
-        const u64 pbase_next = pbase + kStepAdvance;
-        const u64 m0_next = st + 1 < s_end ? rng_mix(pbase_next) >> 11 : 0;
         const bool spiked = neuron_advance_step<R>(
             rc, ns, pk, EXC, n, ((ex_mask >> st) & 1u) ? ex_acc[st] : zero, ((in_mask >> st) & 1u) ? in_acc[st] : zero,
-            refresh, sic_input ? sic_acc[st] : zero, has_noise, noise, pbase, m0, ex_decay, in_decay);
-        pbase = pbase_next;
-        m0 = m0_next;
+            refresh, sic_input ? sic_acc[st] : zero, has_noise, noise, pbase, ex_decay, in_decay);
+        pbase += kStepAdvance;
         ++since;
         if (++phase == si) phase = 0;
         if (++nphase == spn) {
@@ -270,19 +264,14 @@ __device__ __forceinline__ void window_cells(const RunConsts& rc, const NetScala
             R factor = static_cast<R>(0.0);
             u64 pbase = step_base(ns.seed, kAstroPoissonKey, win_start + s_begin, a);
             u64 nbase = step_base(ns.seed, kAstroNoiseKey, win_start + s_begin, a);
-            // each step's first draws are hashed during the step before
-            AstroDraws dr = astro_draws(pbase, nbase);
             // recording phase (t + 1) % rec_every, advanced by a counter
             i64 rphase = p.ca_rec ? (win_start + s_begin + 1) % p.rec_every : 1;
             for (int st = s_begin; st < s_end; ++st) {
                 const i64 t = win_start + st;
-                const u64 pb_next = pbase + kStepAdvance, nb_next = nbase + kStepAdvance;
-                const AstroDraws dr_next = st + 1 < s_end ? astro_draws(pb_next, nb_next) : AstroDraws{0, 0, 0};
                 factor = astro_advance_step<R>(rc, ns, s, ((in_mask >> st) & 1u) ? acc[st] : static_cast<R>(0.0), a, t,
-                                               pbase, nbase, dr);
-                pbase = pb_next;
-                nbase = nb_next;
-                dr = dr_next;
+                                               pbase, nbase);
+                pbase += kStepAdvance;
+                nbase += kStepAdvance;
                 if (p.ca_rec) {
                     record_ca<R>(p, a, t, rphase == 0, s.Ca);
                     if (++rphase == p.rec_every) rphase = 0;
