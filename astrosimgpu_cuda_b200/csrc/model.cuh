@@ -184,13 +184,14 @@ struct NeuronK {
     float f_gL_DT, f_inv_DT, f_inv_Cm, f_inv_tauw;
     // Float copies read by the FP32 stages (converted once here, not per use).
     float f_V_peak, f_E_L, f_V_th, f_E_ex, f_E_in, f_g_L, f_I_e, f_a, f_psc_init_ex, f_psc_init_in;
-    // The FP32 form's AdEx right-hand side refolded (adex_rhs_folded):
-    //   dV = A Vc + B - w / C_m + 2^(K1 Vc + K2),  A = A0 - (g_ex + g_in) / C_m,
-    //   B = C0 + (g_ex E_ex + g_in E_in + I_ext) / C_m,   dw = Wa Vc + Wb - w / tau_w,
-    // with K1 = log2(e) / Delta_T, K2 = log2(g_L Delta_T / C_m) - K1 V_th, A0 = -g_L / C_m,
-    // C0 = (g_L E_L + I_e) / C_m, Eex_c = E_ex / C_m, Ein_c = E_in / C_m, Wa = a / tau_w,
-    // Wb = -a E_L / tau_w (each computed in double, rounded once).
-    float f_K1, f_K2, f_A0, f_C0, f_Eex_c, f_Ein_c, f_Wa, f_Wb;
+    // The FP32 form's AdEx right-hand side refolded (adex_rhs_folded), around E_L and
+    // V_th so that no two large terms cancel:  with u = Vc - E_L,
+    //   dV = A u + B - w / C_m + 2^(K1 (Vc - V_th) + K2),  A = A0 - (g_ex + g_in) / C_m,
+    //   B = C0 + (g_ex Eex_c + g_in Ein_c) + I_ext / C_m,   dw = Wa u - w / tau_w,
+    // with K1 = log2(e) / Delta_T, K2 = log2(g_L Delta_T / C_m), A0 = -g_L / C_m,
+    // C0 = I_e / C_m, Eex_c = (E_ex - E_L) / C_m, Ein_c = (E_in - E_L) / C_m and
+    // Wa = a / tau_w (each computed in double, rounded once).
+    float f_K1, f_K2, f_A0, f_C0, f_Eex_c, f_Ein_c, f_Wa, f_pad2;
     // Refractory length in steps, static_cast<int>(t_ref / h_step + 0.5) (src/astrosim_fused.cu:555);
     // set with the step size.
     int ref_steps;
@@ -296,13 +297,13 @@ inline NeuronK neuron_constants(const Biology& b, bool exc) {  // src/astrosim_f
         const double log2e = 1.4426950408889634073599246810019;
         const double K1 = log2e / k.Delta_T;
         k.f_K1 = static_cast<float>(K1);
-        k.f_K2 = static_cast<float>(std::log2(k.g_L * k.Delta_T / k.C_m) - K1 * k.V_th);
+        k.f_K2 = static_cast<float>(std::log2(k.g_L * k.Delta_T / k.C_m));
         k.f_A0 = static_cast<float>(-k.g_L / k.C_m);
-        k.f_C0 = static_cast<float>((k.g_L * k.E_L + k.I_e) / k.C_m);
-        k.f_Eex_c = static_cast<float>(k.E_ex / k.C_m);
-        k.f_Ein_c = static_cast<float>(k.E_in / k.C_m);
+        k.f_C0 = static_cast<float>(k.I_e / k.C_m);
+        k.f_Eex_c = static_cast<float>((k.E_ex - k.E_L) / k.C_m);
+        k.f_Ein_c = static_cast<float>((k.E_in - k.E_L) / k.C_m);
         k.f_Wa = static_cast<float>(k.a / k.tau_w);
-        k.f_Wb = static_cast<float>(-k.a * k.E_L / k.tau_w);
+        k.f_pad2 = 0.0f;
     }
     k.ref_steps = 0;
     k.rcp_C_m = 1.0 / k.C_m;
@@ -451,7 +452,8 @@ __device__ __forceinline__ void neuron_rhs(const NeuronK& p, float V, float w, f
 
 #ifndef ASTROSIM_FP32_IEEE
 // The conductance-dependent part of the FP32 form's refolded AdEx right-hand side:
-// dV = A Vc + B - w / C_m + 2^(K1 Vc + K2) (see NeuronK).  `iext_c` = C0 + I_ext / C_m.
+// dV = A (Vc - E_L) + B - w / C_m + 2^(K1 (Vc - V_th) + K2) (see NeuronK).
+// `iext_c` = C0 + I_ext / C_m.
 struct AdexCoef {
     float A, B;
 };
@@ -464,8 +466,9 @@ __device__ __forceinline__ AdexCoef adex_coef(const NeuronK& p, float g_ex, floa
 __device__ __forceinline__ void adex_rhs_folded(const NeuronK& p, const AdexCoef& c, float V, float w, float& dV,
                                                 float& dw) {
     const float Vc = fminf(V, p.f_V_peak);
-    dV = fmaf(c.A, Vc, fmaf(-p.f_inv_Cm, w, c.B)) + ex2_ftz(fmaf(Vc, p.f_K1, p.f_K2));
-    dw = fmaf(p.f_Wa, Vc, fmaf(-p.f_inv_tauw, w, p.f_Wb));
+    const float u = Vc - p.f_E_L;
+    dV = fmaf(c.A, u, fmaf(-p.f_inv_Cm, w, c.B)) + ex2_ftz(fmaf(Vc - p.f_V_th, p.f_K1, p.f_K2));
+    dw = fmaf(p.f_Wa, u, -p.f_inv_tauw * w);
 }
 #endif
 

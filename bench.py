@@ -43,8 +43,8 @@ PRE_MS, SIM_MS = 100.0, 500.0
 # slots busy.  Bytes and instructions grow with the cell count, so a launch at N
 # carries about N / 3e6 times these.
 PROFILED_WINDOW = {
-    "fp32": {"n": 3_000_000, "dram": None, "warp_inst": None, "issue_busy": None},
-    "fp64": {"n": 3_000_000, "dram": None, "warp_inst": None, "issue_busy": None},
+    "fp32": {"n": 3_000_000, "dram": 353.47e6, "warp_inst": 376.78e6, "issue_busy": 0.844},
+    "fp64": {"n": 3_000_000, "dram": 506.90e6, "warp_inst": 838.86e6, "issue_busy": 0.736},
 }
 PROFILED_SOURCE = "ncu, one steady-state window_kernel launch at N_total=3e6 (profiles/), scaled to N_total"
 SCHEDULERS_PER_SM = 4  # warp schedulers per B200 SM: one warp instruction each per cycle at most
