@@ -264,8 +264,14 @@ struct Remerge {
     long long k;       // table-orbit index where the exact walk rejoins (-1: section ended first)
     long long shift;   // true index - table index after rejoining
     u32 m;             // explicit pre starts recorded
-    u32 ok;
+    u32 ok;            // the walk rejoined or reached the section's end
     u64 end;           // section end when the walk reached the last pre
+    // a walk that recorded its cap of starts first (ok == 0, capped == 1): the start
+    // and true index of its next pre, from which it can be continued
+    u64 c_next;
+    long long r_next;
+    u32 capped;
+    u32 pad_;
 };
 
 __device__ __forceinline__ long long find_in_orbit(const u64* orbit, u64 n, u64 c) {
@@ -277,44 +283,63 @@ __device__ __forceinline__ long long find_in_orbit(const u64* orbit, u64 n, u64 
     return (lo < n && orbit[lo] == c) ? static_cast<long long>(lo) : -1;
 }
 
-// For each hazard, assume it is real (true index = r + d) and walk exactly from
-// there, applying the autapse rule with true indices, until the walk lands on a
-// start of the table orbit (or the section's last pre ends).
-__global__ void remerge_kernel(Sec s, const Hazard* hz, u32 n_hz, const u64* orbit, u64 n_orbit, u64 n_pres,
-                               u32 max_explicit, u64* expl, Remerge* res) {
-    const u32 h = blockIdx.x * blockDim.x + threadIdx.x;
-    if (h >= n_hz) return;
-    Remerge out{-1, 0, 0, 0, 0};
-    long long r = static_cast<long long>(hz[h].r) + hz[h].d;
-    if (r < 0 || r >= static_cast<long long>(n_pres)) {
-        res[h] = out;
-        return;
-    }
-    u64 c = orbit[hz[h].r];
-    u64* mine = expl + static_cast<u64>(h) * max_explicit;
-    mine[out.m++] = c;
+// The exact walk from pre start c with true index r, applying the autapse rule
+// with true indices, until it lands on a start of the table orbit, the section's
+// last pre ends, or it has recorded `cap` starts (then it stops where it stands and
+// can be continued from there).
+__device__ __forceinline__ void remerge_from(const Sec& s, u64 c, long long r, const u64* orbit, u64 n_orbit,
+                                             u64 n_pres, u32 cap, u64* starts, Remerge& out) {
+    out = Remerge{-1, 0, 0, 0, 0, 0, 0, 0, 0};
+    starts[out.m++] = c;
     for (;;) {
         c = walk_pre_end(s, c, static_cast<u32>(r));
         ++r;
         if (r >= static_cast<long long>(n_pres)) {
             out.end = c;
             out.ok = 1;
-            break;
+            return;
         }
         const long long k = find_in_orbit(orbit, n_orbit, c);
         if (k >= 0) {
             out.k = k;
             out.shift = r - k;
             out.ok = 1;
-            break;
+            return;
         }
-        if (out.m >= max_explicit) {
-            atomicOr(s.err, kErrExplicit);
-            break;
+        if (out.m >= cap) {
+            out.capped = 1;
+            out.c_next = c;
+            out.r_next = r;
+            return;
         }
-        mine[out.m++] = c;
+        starts[out.m++] = c;
     }
+}
+
+// For each hazard, assume it is real (true index = r + d) and walk exactly from
+// there (remerge_from) with at most max_explicit starts.  Most walks rejoin within a
+// few pres; the host continues a capped walk only when its replay reaches it.
+__global__ void remerge_kernel(Sec s, const Hazard* hz, u32 n_hz, const u64* orbit, u64 n_orbit, u64 n_pres,
+                               u32 max_explicit, u64* expl, Remerge* res) {
+    const u32 h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= n_hz) return;
+    const long long r = static_cast<long long>(hz[h].r) + hz[h].d;
+    if (r < 0 || r >= static_cast<long long>(n_pres)) {
+        res[h] = Remerge{-1, 0, 0, 0, 0, 0, 0, 0, 0};
+        return;
+    }
+    Remerge out;
+    remerge_from(s, orbit[hz[h].r], r, orbit, n_orbit, n_pres, max_explicit, expl + static_cast<u64>(h) * max_explicit,
+                 out);
     res[h] = out;
+}
+
+// One capped walk continued from where it stopped.
+__global__ void remerge_continue_kernel(Sec s, u64 c, long long r, const u64* orbit, u64 n_orbit, u64 n_pres, u32 cap,
+                                        u64* starts, Remerge* res) {
+    Remerge out;
+    remerge_from(s, c, r, orbit, n_orbit, n_pres, cap, starts, out);
+    *res = out;
 }
 
 __global__ void copy_orbit_kernel(const u64* src, u64* dst, u64 n) {
@@ -464,12 +489,12 @@ Status section_orbit(const SectionPlan& P, Sec s, u64 start, DevBuf<int>& err, D
     }
     double slack = 1.04;
     int K = 32;
-    // Explicit pre starts kept per re-merge walk.  Walks rejoin after a median of 2
-    // pres and at most about 900 in every network measured (N = 2e3-1e6); a longer
-    // one flags kErrExplicit and the section runs again with 8x the room.  A small
-    // buffer stays in the stream-ordered pool: at 8192 starts for ~5,200 hazards it
-    // took 340 MB from cudaMalloc, whose free stalls every concurrent build.
-    u32 max_explicit = 1024;
+    // Explicit pre starts kept per speculative re-merge walk.  Walks rejoin after a
+    // median of 2 pres (at most about 900 in every network measured, N = 2e3-1e6),
+    // and the replay uses only the 50-90 on its chain of about 5,200; so every walk
+    // stops at 64 starts and the replay continues, one at a time, the capped walks it
+    // reaches.  The kernel then waits for 64 pres instead of the longest walk.
+    const u32 max_explicit = 64;
     PhaseClock pc(st);
     for (int attempt = 0; attempt < 8; ++attempt) {
         AS_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(int), st));
@@ -585,16 +610,15 @@ Status section_orbit(const SectionPlan& P, Sec s, u64 start, DevBuf<int>& err, D
             AS_CUDA(cudaGetLastError());
             AS_TRY(to_host(rr.data(), rm.get(), n_hz, st));
             AS_TRY(read_err(err, &herr, st));
-            if ((herr & kErrExplicit) && max_explicit < (1u << 20)) {
-                max_explicit *= 8;
-                continue;
-            }
             if (herr) return make_error(ASTROSIM_ERR_UNSUPPORTED, "%s: re-merge walks failed (flags %d)", P.name, herr);
         }
         pc.mark("  re-merge walks");
         // replay the hazards in order with the running shift (true index - table index)
-        struct Piece { bool expl; u64 t_start, src, len; };
+        struct Piece { const u64* src; u64 t_start, len; };
         std::vector<Piece> pieces;
+        std::vector<DevBuf<u64>> cont_starts;  // starts of the capped walks the replay continued
+        DevBuf<Remerge> cont_res;
+        AS_TRY(cont_res.alloc(1));
         long long d = 0;
         u64 cur_f = 0, cur_t = 0;
         bool ended = false;
@@ -604,18 +628,37 @@ Status section_orbit(const SectionPlan& P, Sec s, u64 start, DevBuf<int>& err, D
             const Hazard& h = hh[i];
             if (h.r < cur_f || h.d != d) continue;
             if (static_cast<long long>(h.r) + d >= static_cast<long long>(P.n_pres)) break;  // past the section
-            const Remerge& m = rr[i];
-            if (!m.ok) return make_error(ASTROSIM_ERR_CUDA, "%s: re-merge walk incomplete", P.name);
-            if (h.r > cur_f) pieces.push_back(Piece{false, cur_t, cur_f, h.r - cur_f});
+            Remerge m = rr[i];
+            if (h.r > cur_f) pieces.push_back(Piece{forbit.get() + cur_f, cur_t, h.r - cur_f});
             const u64 t_autapse = static_cast<u64>(static_cast<long long>(h.r) + d);
-            pieces.push_back(Piece{true, t_autapse, static_cast<u64>(i) * max_explicit, m.m});
+            pieces.push_back(Piece{expl.get() + static_cast<u64>(i) * max_explicit, t_autapse, m.m});
+            u64 walked = m.m;
+            for (u32 cap = 4096; m.capped;) {  // this walk is on the chain: continue it
+                DevBuf<u64> buf;
+                AS_TRY(buf.alloc(cap));
+                remerge_continue_kernel<<<1, 1, 0, st>>>(s, m.c_next, m.r_next, forbit.get(), target, P.n_pres, cap,
+                                                         buf.get(), cont_res.get());
+                AS_CUDA(cudaGetLastError());
+                Remerge m2{};
+                AS_TRY(to_host(&m2, cont_res.get(), 1, st));
+                if (m2.capped && cap < (1u << 24)) {
+                    cap *= 8;  // the same continuation again with more room
+                    continue;
+                }
+                pieces.push_back(Piece{buf.get(), t_autapse + walked, m2.m});
+                walked += m2.m;
+                cont_starts.push_back(std::move(buf));
+                m = m2;
+                break;
+            }
+            if (!m.ok) return make_error(ASTROSIM_ERR_CUDA, "%s: re-merge walk incomplete", P.name);
             if (m.k < 0) {
                 ended = true;
                 end_pos = m.end;
-                cur_t = t_autapse + m.m;
+                cur_t = t_autapse + walked;
                 break;
             }
-            cur_t = t_autapse + m.m;
+            cur_t = t_autapse + walked;
             cur_f = static_cast<u64>(m.k);
             d = m.shift;
             if (d < -K || d > K) { shift_overflow = true; break; }
@@ -624,7 +667,7 @@ Status section_orbit(const SectionPlan& P, Sec s, u64 start, DevBuf<int>& err, D
         if (!ended) {
             const u64 len = P.n_pres - cur_t;
             if (cur_f + len > target) { K *= 4; continue; }  // needed table orbit beyond the margin
-            if (len) pieces.push_back(Piece{false, cur_t, cur_f, len});
+            if (len) pieces.push_back(Piece{forbit.get() + cur_f, cur_t, len});
             cur_t += len;
         }
         if (cur_t != P.n_pres) return make_error(ASTROSIM_ERR_CUDA, "%s: spliced orbit has %llu of %llu pres", P.name,
@@ -632,8 +675,7 @@ Status section_orbit(const SectionPlan& P, Sec s, u64 start, DevBuf<int>& err, D
                                                  static_cast<unsigned long long>(P.n_pres));
         AS_TRY(orbit.alloc(P.n_pres));
         for (const Piece& pc : pieces) {
-            const u64* src = pc.expl ? expl.get() + pc.src : forbit.get() + pc.src;
-            copy_orbit_kernel<<<ceil_div(pc.len, 256), 256, 0, st>>>(src, orbit.get() + pc.t_start, pc.len);
+            copy_orbit_kernel<<<ceil_div(pc.len, 256), 256, 0, st>>>(pc.src, orbit.get() + pc.t_start, pc.len);
             AS_CUDA(cudaGetLastError());
         }
         if (ended) {

@@ -16,8 +16,7 @@ enum ErrBits : int {
     kErrCache = 1,     // a walk left the skip cache
     kErrHash = 2,      // claim table full
     kErrDelta = 4,     // an entry fell outside the candidate window
-    kErrOrbit = 8,     // materialised chunk did not meet its successor (internal)
-    kErrExplicit = 16  // re-merge walk longer than its buffer
+    kErrOrbit = 8      // materialised chunk did not meet its successor (internal)
 };
 
 struct Sec {
