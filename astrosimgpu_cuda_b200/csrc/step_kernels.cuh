@@ -301,21 +301,27 @@ __device__ __forceinline__ bool neuron_advance_step(const RunConsts& rc, const N
 }
 
 // Tsodyks-Markram update of a presynaptic neuron at its spike (src/astrosim_fused.cu:564-579);
-// returns the multiplier its outgoing synapses carry.
+// returns the multiplier its outgoing synapses carry.  Every operation's rounding is
+// written out, because the compiler's choice of which multiply-adds to fuse here
+// varied between launch-bounds instantiations of the window kernel (one fused
+// step * dt - t_last; measured on every spike of a run with facilitation): these are
+// the roundings the per-step kernel computes, so every engine and variant gives
+// the same bits.  x = 1 + (x - x u - 1) x_decay with x - x u and the last
+// multiply-add fused; u = U + (u (1 - U)) u_decay with the last one fused.
 template <typename R>
 __device__ __forceinline__ R stp_on_spike(const RunConsts& rc, R& sx, R& su, double& st, i64 step) {
     if (!rc.stp_enabled) return static_cast<R>(1.0);
     double x = static_cast<double>(sx), u = static_cast<double>(su);
-    const double t_now = static_cast<double>(step) * rc.dt;
-    const double elapsed = t_now - st;
-    const double x_decay = exp(-elapsed / rc.stp_tau_rec);
-    const double u_decay = rc.stp_tau_fac < 1e-10 ? 0.0 : exp(-elapsed / rc.stp_tau_fac);
-    x = 1.0 + (x - x * u - 1.0) * x_decay;
-    u = rc.stp_U + u * (1.0 - rc.stp_U) * u_decay;
+    const double t_now = __dmul_rn(static_cast<double>(step), rc.dt);
+    const double elapsed = __dsub_rn(t_now, st);
+    const double x_decay = exp(__ddiv_rn(-elapsed, rc.stp_tau_rec));
+    const double u_decay = rc.stp_tau_fac < 1e-10 ? 0.0 : exp(__ddiv_rn(-elapsed, rc.stp_tau_fac));
+    x = __fma_rn(__dsub_rn(__fma_rn(-x, u, x), 1.0), x_decay, 1.0);
+    u = __fma_rn(__dmul_rn(u, __dsub_rn(1.0, rc.stp_U)), u_decay, rc.stp_U);
     sx = static_cast<R>(x);
     su = static_cast<R>(u);
     st = t_now;
-    return static_cast<R>(x * u);
+    return static_cast<R>(__dmul_rn(x, u));
 }
 
 // noise_std * N(0,1) of neuron j for noise index idx (src/astrosim_fused.cu:494-504).
