@@ -105,3 +105,29 @@ def test_active_astrocytes_windowed_matches_per_step(monkeypatch, precision, sic
             np.testing.assert_array_equal(s.spike_counts(), ref["counts"])
     monkeypatch.delenv("ASTROSIM_PUSH_LIMIT", raising=False)
     assert ref_active >= min_active, ref_active
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_every_variant_bit_identical_with_facilitation_and_active_astrocytes(monkeypatch, precision):
+    """The regime where the launch-bounds instantiations once rounded the Tsodyks-
+    Markram update differently (one fused step * dt - t_last): strong SIC input makes
+    neurons fire often, and facilitation (U = 0.3, tau_fac = 150 ms) makes u vary.
+    Every variant gives the per-step path's results bit for bit."""
+    bio = {"SIC_th": 0.06, "w_a2n": 3.0, "stp_U": 0.3, "stp_tau_fac": 150.0}
+    kw = dict(n_total=6000, seed=13, pre_ms=10, sim_ms=50, precision=precision)
+    monkeypatch.setenv("ASTROSIM_STEPPER", "plain")
+    with asg.Simulation(biology=bio, **kw) as s:
+        s.step(600)
+        ref = {k: s.state(k) for k in STATES}
+        ref["counts"] = s.spike_counts()
+    assert ref["counts"].sum() > 5000
+    monkeypatch.setenv("ASTROSIM_STEPPER", "auto")
+    for v in range(9):
+        monkeypatch.setenv("ASTROSIM_WINDOW_VARIANT", str(v))
+        with asg.Simulation(biology=bio, **kw) as s:
+            for c in (7, 3, 290, 300):
+                s.step(c)
+            for k in STATES:
+                np.testing.assert_array_equal(s.state(k), ref[k], err_msg=f"{k} variant {v}")
+            np.testing.assert_array_equal(s.spike_counts(), ref["counts"], err_msg=f"variant {v}")
+    monkeypatch.delenv("ASTROSIM_WINDOW_VARIANT", raising=False)
