@@ -16,10 +16,11 @@
 //     can reach, computed once; ambiguous values (quotient within a few ulps of an
 //     integer) are settled with the host C library that the reference uses.
 //  3. For each walk section (E block, I block, inhibitory pres), the section's
-//     tape is cut into chunks.  For each chunk, one CTA walks from EVERY candidate
+//     tape is cut into chunks.  For each chunk, walks start from EVERY candidate
 //     entry position in [T, T + delta) -- the chunk's first pre start must be one
-//     of them -- merging walks that land on the same pre start (a shared-memory
-//     claim table).  That gives an exact table: entry -> (exit, pres started).
+//     of them -- and merge when they land on the same pre start (a claim table):
+//     one CTA per short chunk, all candidates at once; persistent warp swarms for
+//     long chunks.  That gives an exact table: entry -> (exit, pres started).
 //     Tables are composed (groups in parallel, then one thread over the groups),
 //     which yields every chunk's true entry, and one thread per chunk then writes
 //     every pre's start ("orbit").
@@ -32,14 +33,18 @@
 //     shift and splices the true orbit.
 //  5. Count and emit: one thread per pre walks its row again (exact rules,
 //     including autapses), first counting, then writing edges at scanned offsets.
-//     The lists are in emission order; the stable radix sort of builder.cu turns
-//     them into the target-keyed CSRs.
+//     The lists are in emission order (the two excitatory blocks interleaved by pre,
+//     which makes the excitatory list source-major); the stable radix sort of
+//     builder.cu turns them into the target-keyed CSRs, and the exc and inh lists
+//     are kept as the windowed engine's forward lists.
 // Every step is exact; the outcome is bit-identical to the sequential walk.
 
 #include <cub/device/device_scan.cuh>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <map>
 #include <vector>
 
@@ -72,6 +77,33 @@ __global__ void pool_pass_kernel(u64 seed, u32 n_neurons, u32 n_astro, u32 take,
     const u64 c0 = c;
     pool_one(seed, n_astro, c, pool + static_cast<u64>(q) * kPoolSize);
     extra[q] = c - c0 - take;
+}
+
+// Tape positions where a pool started there needs redraws (a duplicate pick), with
+// the number of extra draws: every t in [t0, t0 + n).
+struct PoolRedraw {
+    u64 t;
+    u32 extra, pad_;
+};
+
+__global__ void pool_redraw_kernel(u64 seed, u32 n_astro, u32 take, u64 t0, u64 n, PoolRedraw* out, unsigned* count,
+                                   unsigned cap) {
+    const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
+    u32 pl[kPoolSize];
+    for (u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+        u64 c = t0 + i;
+        pool_one(seed, n_astro, c, pl);
+        const u64 extra = c - (t0 + i) - take;
+        if (extra) {
+            const unsigned k = atomicAdd(count, 1u);
+            if (k < cap) out[k] = PoolRedraw{t0 + i, static_cast<u32>(extra), 0u};
+        }
+    }
+}
+
+__global__ void scatter_extra_kernel(const u32* q, const u32* e, u32 n, u64* extra) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) extra[q[i]] = e[i];
 }
 
 __global__ void diff_kernel(const u64* a, const u64* b, u64 n, int* flag) {
@@ -150,6 +182,164 @@ __global__ void table_kernel(Sec s, u64 sec_start, u32 chunk_len, u32 delta, u64
         t_exit[static_cast<u64>(blockIdx.x) * delta + w] = ex[x];
         t_cnt[static_cast<u64>(blockIdx.x) * delta + w] = static_cast<u32>(total);
     }
+}
+
+// ---------------------------------------------------------------- chunk tables by warp swarms
+// The same tables from persistent warps.  In the one-CTA-per-chunk form above, the
+// walk that never merges holds its CTA (delta threads, 42 KB of shared memory) for
+// the whole chunk, so an SM keeps only 5 chunks in flight and, late in each chunk,
+// walks 5-10 chains.  Here a warp takes a chunk, its lanes take the candidates a few
+// at a time (a lane whose walk merged or left the chunk takes the next candidate),
+// claims go to a per-warp table in global memory, and once every candidate has
+// started and at most kSwarmHandoff walks remain, the warp hands them to a
+// one-thread-per-walk kernel and takes the next chunk.  A walk's exit and count are
+// the same whoever it merges into, so the tables are identical.
+constexpr u32 kSwarmSlots = 4096;  // claim slots per warp (32 KB of global memory)
+constexpr u32 kSwarmHandoff = 4;
+constexpr u32 kSwarmIdle = 0xFFFFFFFFu;
+
+struct SwarmRec {
+    int* par;     // walk this one merged into, -1 for a walk that reached the chunk end
+    u32* mycnt;   // pres walked before merging (or in all)
+    u32* pcnt;    // the merged-into walk's count where they met
+    u64* ex;      // where the walk stopped
+};
+
+struct SwarmCont {
+    u32 chunk, w;
+    u64 c;
+    u32 cnt, pad_;
+};
+
+__global__ void __launch_bounds__(128) swarm_kernel(Sec s, u64 sec_start, u32 chunk_len, u32 delta, u32 n_chunks,
+                                                    unsigned* next_chunk, unsigned long long* tables, SwarmRec rec,
+                                                    SwarmCont* cont, unsigned* n_cont, unsigned cont_cap) {
+    const u32 lane = threadIdx.x & 31u;
+    const u64 warp = (static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    unsigned long long* tab = tables + warp * kSwarmSlots;
+    NoVisit nv;
+    for (;;) {
+        u32 chunk = 0;
+        if (lane == 0) chunk = atomicAdd(next_chunk, 1u);
+        chunk = __shfl_sync(0xffffffffu, chunk, 0);
+        if (chunk >= n_chunks) return;
+        for (u32 i = lane; i < kSwarmSlots; i += 32) tab[i] = kEmpty;
+        __threadfence();  // the cleared slots are in place before any lane's first claim
+        __syncwarp();
+        const u64 T0 = sec_start + static_cast<u64>(chunk) * chunk_len, T1 = T0 + chunk_len;
+        const u64 rb = static_cast<u64>(chunk) * delta;
+        u32 w = lane < delta ? lane : kSwarmIdle;
+        u64 c = T0 + lane;
+        u32 cnt = 0;
+        u32 next = min(32u, delta);
+        for (;;) {
+            bool claimed = false;
+            if (w != kSwarmIdle) {
+                if (c >= T1) {  // reached the chunk end
+                    rec.par[rb + w] = -1;
+                    rec.mycnt[rb + w] = cnt;
+                    rec.ex[rb + w] = c;
+                    w = kSwarmIdle;
+                } else {
+                    const u32 key = static_cast<u32>(c - T0);
+                    u32 slot = (key * 2654435761u) & (kSwarmSlots - 1);
+                    const unsigned long long mine = (static_cast<unsigned long long>(key) << 32) |
+                                                    (static_cast<unsigned long long>(w) << 22) | cnt;
+                    for (u32 probe = 0;; ++probe) {
+                        const unsigned long long old = atomicCAS(&tab[slot], kEmpty, mine);
+                        if (old == kEmpty) {  // claimed: this walk continues from here
+                            claimed = true;
+                            break;
+                        }
+                        if (static_cast<u32>(old >> 32) == key) {  // another walk was here: follow it
+                            rec.par[rb + w] = static_cast<int>((old >> 22) & 0x3FFu);
+                            rec.pcnt[rb + w] = static_cast<u32>(old & 0x3FFFFFu);
+                            rec.mycnt[rb + w] = cnt;
+                            rec.ex[rb + w] = c;
+                            w = kSwarmIdle;
+                            break;
+                        }
+                        slot = (slot + 1) & (kSwarmSlots - 1);
+                        if (probe + 1 >= kSwarmSlots) {  // table full: the host retries with shorter chunks
+                            atomicOr(s.err, kErrHash);
+                            rec.par[rb + w] = -1;
+                            rec.mycnt[rb + w] = cnt;
+                            rec.ex[rb + w] = c;
+                            w = kSwarmIdle;
+                            break;
+                        }
+                    }
+                }
+            }
+            // idle lanes take the next candidates (they claim their start in the next round)
+            const unsigned idle = __ballot_sync(0xffffffffu, w == kSwarmIdle);
+            if (next < delta && idle) {
+                const u32 rank = __popc(idle & ((1u << lane) - 1u));
+                if (w == kSwarmIdle && next + rank < delta) {
+                    w = next + rank;
+                    c = T0 + w;
+                    cnt = 0;
+                }
+                next = min(delta, next + static_cast<u32>(__popc(idle)));
+            }
+            const unsigned live = __ballot_sync(0xffffffffu, w != kSwarmIdle);
+            if (live == 0) break;
+            if (next >= delta && static_cast<u32>(__popc(live)) <= kSwarmHandoff) {
+                if (w != kSwarmIdle) {
+                    const unsigned k = atomicAdd(n_cont, 1u);
+                    if (k < cont_cap) cont[k] = SwarmCont{chunk, w, c, cnt, 0u};
+                    else atomicOr(s.err, kErrOrbit);
+                }
+                break;
+            }
+            if (claimed) {
+                c = walk_pre(s, c, kNoSelf, nv);
+                ++cnt;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// The walks a warp handed off, to the chunk end without claims.
+__global__ void swarm_continue_kernel(Sec s, u64 sec_start, u32 chunk_len, u32 delta, const SwarmCont* cont,
+                                      const unsigned* n_cont, unsigned cont_cap, SwarmRec rec) {
+    const u32 k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= min(*n_cont, cont_cap)) return;
+    const SwarmCont q = cont[k];
+    const u64 T1 = sec_start + static_cast<u64>(q.chunk + 1) * chunk_len;
+    u64 c = q.c;
+    u32 cnt = q.cnt;
+    NoVisit nv;
+    while (c < T1) {
+        c = walk_pre(s, c, kNoSelf, nv);
+        ++cnt;
+    }
+    const u64 r = static_cast<u64>(q.chunk) * delta + q.w;
+    rec.par[r] = -1;
+    rec.mycnt[r] = cnt;
+    rec.ex[r] = c;
+}
+
+// Exit and pre count of every candidate: along its merge chain, the sum of (pres
+// before the merge - the merged-into walk's count there), plus the last walk's count.
+__global__ void swarm_resolve_kernel(u32 delta, u64 n, SwarmRec rec, int* err, u64* t_exit, u32* t_cnt) {
+    const u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const u64 base = i - i % delta;
+    u64 x = i;
+    long long total = 0;
+    for (u32 guard = 0; rec.par[x] >= 0; ++guard) {
+        if (guard >= delta) {  // merges point to earlier claims, so chains cannot cycle
+            atomicOr(err, kErrOrbit);
+            break;
+        }
+        total += static_cast<long long>(rec.mycnt[x]) - static_cast<long long>(rec.pcnt[x]);
+        x = base + static_cast<u32>(rec.par[x]);
+    }
+    total += rec.mycnt[x];
+    t_exit[i] = rec.ex[x];
+    t_cnt[i] = static_cast<u32>(total);
 }
 
 // Composes the tables of kGroup consecutive chunks: thread d follows candidate d.
@@ -274,12 +464,29 @@ struct Remerge {
     u32 pad_;
 };
 
-__device__ __forceinline__ long long find_in_orbit(const u64* orbit, u64 n, u64 c) {
-    u64 lo = 0, hi = n;
-    while (lo < hi) {
+// Index of c in the sorted orbit, or -1.  `from` is a lower bound of where c can be
+// (the previous query's answer: a walk's queries only move forward); the search
+// gallops from there, so a walk that keeps pace with the orbit costs one or two
+// loads per query instead of a full binary search.  `from` becomes c's lower bound.
+__device__ __forceinline__ long long find_in_orbit(const u64* orbit, u64 n, u64 c, u64& from) {
+    u64 lo = from, hi = n;
+    if (lo < n && orbit[lo] < c) {
+        u64 step = 1;
+        hi = lo + 1;
+        while (hi < n && orbit[hi] < c) {
+            lo = hi;
+            step *= 2;
+            hi = lo + step < n ? lo + step : n;
+        }
+        ++lo;  // orbit[lo - 1] < c
+    } else {
+        hi = lo;
+    }
+    while (lo < hi) {  // the first index in [lo, hi) with orbit[index] >= c
         const u64 mid = (lo + hi) >> 1;
         if (orbit[mid] < c) lo = mid + 1; else hi = mid;
     }
+    from = lo;
     return (lo < n && orbit[lo] == c) ? static_cast<long long>(lo) : -1;
 }
 
@@ -291,6 +498,15 @@ __device__ __forceinline__ void remerge_from(const Sec& s, u64 c, long long r, c
                                              u64 n_pres, u32 cap, u64* starts, Remerge& out) {
     out = Remerge{-1, 0, 0, 0, 0, 0, 0, 0, 0};
     starts[out.m++] = c;
+    u64 from = 0;
+    {
+        u64 lo = 0, hi = n_orbit;  // c's lower bound in the orbit, once
+        while (lo < hi) {
+            const u64 mid = (lo + hi) >> 1;
+            if (orbit[mid] < c) lo = mid + 1; else hi = mid;
+        }
+        from = lo;
+    }
     for (;;) {
         c = walk_pre_end(s, c, static_cast<u32>(r));
         ++r;
@@ -299,7 +515,7 @@ __device__ __forceinline__ void remerge_from(const Sec& s, u64 c, long long r, c
             out.ok = 1;
             return;
         }
-        const long long k = find_in_orbit(orbit, n_orbit, c);
+        const long long k = find_in_orbit(orbit, n_orbit, c, from);
         if (k >= 0) {
             out.k = k;
             out.shift = r - k;
@@ -342,9 +558,23 @@ __global__ void remerge_continue_kernel(Sec s, u64 c, long long r, const u64* or
     *res = out;
 }
 
-__global__ void copy_orbit_kernel(const u64* src, u64* dst, u64 n) {
+// The spliced orbit: piece p covers true indices [t_start[p], t_start[p] + len) and
+// is read from src[p]; pieces are in index order and tile [0, n).
+struct OrbitPiece {
+    const u64* src;
+    u64 t_start, len;
+};
+
+__global__ void splice_orbit_kernel(const OrbitPiece* pieces, u32 n_pieces, u64 n, u64* dst) {
     const u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i < n) dst[i] = src[i];
+    if (i >= n) return;
+    u32 lo = 0, hi = n_pieces;  // the last piece with t_start <= i
+    while (hi - lo > 1) {
+        const u32 mid = (lo + hi) >> 1;
+        if (pieces[mid].t_start <= i) lo = mid; else hi = mid;
+    }
+    const OrbitPiece p = pieces[lo];
+    dst[i] = p.src[i - p.t_start];
 }
 
 // ---------------------------------------------------------------- count and emit
@@ -442,6 +672,28 @@ __global__ void section_end_kernel(Sec s, const u64* orbit, u64 last, int self_m
     *end = walk_pre(s, orbit[last], self_post_of(self_mode, static_cast<u32>(last), self_off), nv);
 }
 
+// Excitatory edge layout, source-major: pre r's E-block edges (exc targets) then its
+// I-block edges (inh targets) at fwd_rs[r] = oe_e[r] + oe_i[r] (the two blocks'
+// exclusive scans over the same pres); o_e / o_i (the scans, in place) become each
+// block's emission offsets.  fwd_rs[n] = total.
+__global__ void exc_layout_kernel(u64 n, u64* o_e, u64* o_i, const u64* c_e, u64 total, u32* fwd_rs) {
+    const u64 r = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (r < n) {
+        const u64 base = o_e[r] + o_i[r];
+        fwd_rs[r] = static_cast<u32>(base);
+        o_e[r] = base;
+        o_i[r] = base + c_e[r];
+    }
+    if (r == 0) fwd_rs[n] = static_cast<u32>(total);
+}
+
+// Row starts of a source-major list from its exclusive scan: rs[r] = o[r], rs[n] = total.
+__global__ void rows_from_scan_kernel(u64 n, const u64* o, u64 total, u32* rs) {
+    const u64 r = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (r < n) rs[r] = static_cast<u32>(o[r]);
+    if (r == 0) rs[n] = static_cast<u32>(total);
+}
+
 __global__ void max_row_kernel(const u32* rs, u32 n, unsigned* mx) {
     const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) atomicMax(mx, rs[i + 1] - rs[i]);
@@ -465,6 +717,116 @@ Status to_host(T* dst, const T* src, size_t n, cudaStream_t st) {
 }
 
 Status read_err(const DevBuf<int>& err, int* out, cudaStream_t st) { return to_host(out, err.get(), 1, st); }
+
+// A first guess of the pools' start offsets: prefix[q] = the extra draws of the
+// pools before post q.  Pool q starts at c0 + take * q + prefix[q], and only the
+// positions where a pool would need redraws matter -- about 250 of the 5 nN at any
+// size (a duplicate among 5 picks from nA = N / 5 astrocytes).  They are found in
+// one pass; walking them in order on the host with the running shift gives the
+// offsets.  The fixed-point loop that follows checks the guess (one round when it
+// is right, as it always is unless the list overflowed).
+Status guess_pool_prefix(u64 seed, u32 nN, u32 nA, u32 take, u64 c0, u64* prefix, cudaStream_t st) {
+    if (nN == 0 || take < kPoolSize || static_cast<u64>(take) * 4 >= nA) return Status::Ok();  // no redraws
+    // the positions past the last pool's nominal start: about 4x the expected extra
+    // draws (a pool redraws with probability about 10 / nA)
+    const u64 margin = 4096 + static_cast<u64>(static_cast<double>(nN) * 40.0 / nA);
+    const u64 n = static_cast<u64>(take) * nN + margin;
+    const unsigned cap = 1u << 16;
+    DevBuf<PoolRedraw> list;
+    DevBuf<unsigned> count;
+    AS_TRY(list.alloc(cap));
+    AS_TRY(count.alloc_zero(1, st));
+    pool_redraw_kernel<<<sm_count() * 8, 256, 0, st>>>(seed, nA, take, c0, n, list.get(), count.get(), cap);
+    AS_CUDA(cudaGetLastError());
+    unsigned m = 0;
+    AS_TRY(to_host(&m, count.get(), 1, st));
+    if (m > cap) return Status::Ok();  // leave the zero guess to the loop
+    std::vector<PoolRedraw> h(m);
+    if (m) AS_TRY(to_host(h.data(), list.get(), m, st));
+    std::sort(h.begin(), h.end(), [](const PoolRedraw& a, const PoolRedraw& b) { return a.t < b.t; });
+    std::vector<u32> bq, be;
+    u64 next_start = c0, q_next = 0;
+    for (const PoolRedraw& b : h) {
+        if (b.t < next_start || (b.t - next_start) % take) continue;  // not a pool start
+        const u64 q = q_next + (b.t - next_start) / take;
+        if (q >= nN) break;
+        bq.push_back(static_cast<u32>(q));
+        be.push_back(b.extra);
+        q_next = q + 1;
+        next_start = b.t + take + b.extra;
+    }
+    if (bq.empty()) return Status::Ok();
+    DevBuf<u64> extra;
+    DevBuf<u32> dq, de;
+    AS_TRY(extra.alloc_zero(nN, st));
+    AS_TRY(dq.alloc(bq.size()));
+    AS_TRY(de.alloc(be.size()));
+    AS_CUDA(cudaMemcpyAsync(dq.get(), bq.data(), bq.size() * sizeof(u32), cudaMemcpyHostToDevice, st));
+    AS_CUDA(cudaMemcpyAsync(de.get(), be.data(), be.size() * sizeof(u32), cudaMemcpyHostToDevice, st));
+    scatter_extra_kernel<<<ceil_div(bq.size(), 256), 256, 0, st>>>(dq.get(), de.get(), static_cast<u32>(bq.size()),
+                                                                   extra.get());
+    AS_CUDA(cudaGetLastError());
+    AS_TRY(exclusive_scan_u64(extra.get(), prefix, nN, st));
+    AS_CUDA(cudaStreamSynchronize(st));  // bq / be are host vectors
+    return Status::Ok();
+}
+
+// Resident 128-thread blocks of swarm_kernel per SM, read once.
+u32 swarm_blocks_per_sm() {
+    static std::atomic<int> cached{0};
+    int v = cached.load();
+    if (v > 0) return static_cast<u32>(v);
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, swarm_kernel, 128, 0) != cudaSuccess || nb <= 0) {
+        cudaGetLastError();
+        nb = 8;
+    }
+    cached.store(nb);
+    return static_cast<u32>(nb);
+}
+
+// The (exit, pres) table of every chunk candidate: t_exit/t_cnt[chunk * delta + d]
+// for the walk from tape position sec_start + chunk * chunk_len + d.
+// Long chunks (kSwarmMinChunk positions and up, the sections of networks from about
+// N = 2e5) go to the warp swarms; short ones to one CTA per chunk, which walks all
+// candidates at once and measured faster there (N = 2e3-3e4: 0.3 vs 1.3 ms per
+// section; N = 1e7: 268 ms vs 33 ms for the E block the other way round).
+constexpr u32 kSwarmMinChunk = 16384;
+
+Status chunk_tables(Sec s, u64 sec_start, u32 chunk_len, u32 delta, u32 n_chunks, u64* t_exit, u32* t_cnt,
+                    cudaStream_t st) {
+    if (chunk_len < kSwarmMinChunk) {
+        table_kernel<<<n_chunks, delta, 0, st>>>(s, sec_start, chunk_len, delta, t_exit, t_cnt);
+        AS_CUDA(cudaGetLastError());
+        return Status::Ok();
+    }
+    const u64 n = static_cast<u64>(n_chunks) * delta;
+    const u32 blocks = std::max<u32>(1, std::min<u32>(ceil_div(n_chunks, 4), sm_count() * swarm_blocks_per_sm()));
+    const unsigned cont_cap = n_chunks * kSwarmHandoff;
+    DevBuf<unsigned long long> tables;
+    DevBuf<int> par;
+    DevBuf<u32> mycnt, pcnt;
+    DevBuf<u64> ex;
+    DevBuf<SwarmCont> cont;
+    DevBuf<unsigned> counters;  // next chunk, handed-off walks
+    AS_TRY(tables.alloc(static_cast<u64>(blocks) * 4 * kSwarmSlots));
+    AS_TRY(par.alloc(n));
+    AS_TRY(mycnt.alloc(n));
+    AS_TRY(pcnt.alloc(n));
+    AS_TRY(ex.alloc(n));
+    AS_TRY(cont.alloc(cont_cap));
+    AS_TRY(counters.alloc_zero(2, st));
+    const SwarmRec rec{par.get(), mycnt.get(), pcnt.get(), ex.get()};
+    swarm_kernel<<<blocks, 128, 0, st>>>(s, sec_start, chunk_len, delta, n_chunks, counters.get(), tables.get(), rec,
+                                         cont.get(), counters.get() + 1, cont_cap);
+    AS_CUDA(cudaGetLastError());
+    swarm_continue_kernel<<<ceil_div(cont_cap, 128), 128, 0, st>>>(s, sec_start, chunk_len, delta, cont.get(),
+                                                                  counters.get() + 1, cont_cap, rec);
+    AS_CUDA(cudaGetLastError());
+    swarm_resolve_kernel<<<ceil_div(n, 256), 256, 0, st>>>(delta, n, rec, s.err, t_exit, t_cnt);
+    AS_CUDA(cudaGetLastError());
+    return Status::Ok();
+}
 
 struct SectionPlan {
     const char* name;
@@ -514,8 +876,7 @@ Status section_orbit(const SectionPlan& P, Sec s, u64 start, DevBuf<int>& err, D
         AS_TRY(c_entry.alloc(n_chunks));
         AS_TRY(c_g0.alloc(n_chunks));
         AS_TRY(endg.alloc(1));
-        table_kernel<<<n_chunks, delta, 0, st>>>(s, start, chunk_len, delta, t_exit.get(), t_cnt.get());
-        AS_CUDA(cudaGetLastError());
+        AS_TRY(chunk_tables(s, start, chunk_len, delta, n_chunks, t_exit.get(), t_cnt.get(), st));
         group_compose_kernel<<<n_groups, delta, 0, st>>>(s, start, chunk_len, delta, n_chunks, t_exit.get(),
                                                          t_cnt.get(), g_exit.get(), g_cnt.get());
         AS_CUDA(cudaGetLastError());
@@ -674,9 +1035,18 @@ Status section_orbit(const SectionPlan& P, Sec s, u64 start, DevBuf<int>& err, D
                                                  static_cast<unsigned long long>(cur_t),
                                                  static_cast<unsigned long long>(P.n_pres));
         AS_TRY(orbit.alloc(P.n_pres));
-        for (const Piece& pc : pieces) {
-            copy_orbit_kernel<<<ceil_div(pc.len, 256), 256, 0, st>>>(pc.src, orbit.get() + pc.t_start, pc.len);
+        std::vector<OrbitPiece> table;
+        for (const Piece& pc : pieces)
+            if (pc.len) table.push_back(OrbitPiece{pc.src, pc.t_start, pc.len});
+        if (!table.empty()) {
+            DevBuf<OrbitPiece> dtab;
+            AS_TRY(dtab.alloc(table.size()));
+            AS_CUDA(cudaMemcpyAsync(dtab.get(), table.data(), table.size() * sizeof(OrbitPiece),
+                                    cudaMemcpyHostToDevice, st));
+            splice_orbit_kernel<<<ceil_div(P.n_pres, 256), 256, 0, st>>>(dtab.get(), static_cast<u32>(table.size()),
+                                                                         P.n_pres, orbit.get());
             AS_CUDA(cudaGetLastError());
+            AS_CUDA(cudaStreamSynchronize(st));  // the host table
         }
         if (ended) {
             *end = end_pos;
@@ -710,6 +1080,7 @@ Status build_parallel(const Sizes& sz, u64 seed, u64 c0, Network& net, cudaStrea
     AS_TRY(pool.alloc(static_cast<u64>(nN) * kPoolSize));
     AS_TRY(extra.alloc(nN));
     AS_TRY(prefix.alloc_zero(nN, st));
+    AS_TRY(guess_pool_prefix(seed, nN, nA, take, c0, prefix.get(), st));
     AS_TRY(prefix_new.alloc(nN));
     AS_TRY(flag.alloc(1));
     u64 pools_end = 0;
@@ -803,6 +1174,7 @@ Status build_parallel(const Sizes& sz, u64 seed, u64 c0, Network& net, cudaStrea
     DevBuf<unsigned long long> totals;
     AS_TRY(totals.alloc_zero(6, st));
     u64 tot_e[3] = {0, 0, 0}, tot_a[3] = {0, 0, 0}, tot_s[3] = {0, 0, 0};
+    DevBuf<u64> ce_block0;  // the E block's per-pre primary counts (the exc layout needs them)
     for (int k = 0; k < 3; ++k) {
         const SectionPlan& P = plans[k];
         s.post_count = P.post_count;
@@ -832,7 +1204,29 @@ Status build_parallel(const Sizes& sz, u64 seed, u64 c0, Network& net, cudaStrea
         tot_e[k] = h[0] + h[1];
         tot_a[k] = h[2] + h[3];
         tot_s[k] = h[4] + h[5];
+        if (k == 0) ce_block0 = std::move(ce);
     }
+    // Both excitatory blocks walk the same pres (the exc neurons), so their edges can
+    // be laid out source-major: the list is then the forward exc list itself, and the
+    // target CSR (a stable sort by target) is unchanged, since each target row's
+    // sources all come from one block, in ascending pre order either way.  The
+    // inhibitory section's emission order is already source-major.
+    if (plans[0].n_pres != plans[1].n_pres)
+        return make_error(ASTROSIM_ERR_CUDA, "excitatory blocks over different pres (%llu, %llu)",
+                          static_cast<unsigned long long>(plans[0].n_pres),
+                          static_cast<unsigned long long>(plans[1].n_pres));
+    if (tot_e[0] + tot_e[1] >= (1ull << 32) || tot_e[2] >= (1ull << 32))
+        return make_error(ASTROSIM_ERR_UNSUPPORTED, "more than 2^32 - 1 primary edges in one CSR");
+    DevBuf<u32> fwd_exc_rs, fwd_inh_rs;
+    AS_TRY(fwd_exc_rs.alloc(plans[0].n_pres + 1));
+    AS_TRY(fwd_inh_rs.alloc(plans[2].n_pres + 1));
+    exc_layout_kernel<<<ceil_div(std::max<u64>(1, plans[0].n_pres), 256), 256, 0, st>>>(
+        plans[0].n_pres, oe[0].get(), oe[1].get(), ce_block0.get(), tot_e[0] + tot_e[1], fwd_exc_rs.get());
+    AS_CUDA(cudaGetLastError());
+    rows_from_scan_kernel<<<ceil_div(std::max<u64>(1, plans[2].n_pres), 256), 256, 0, st>>>(
+        plans[2].n_pres, oe[2].get(), tot_e[2], fwd_inh_rs.get());
+    AS_CUDA(cudaGetLastError());
+    ce_block0.release();
     {
         unsigned long long t[6];
         AS_TRY(to_host(t, totals.get(), 6, st));
@@ -859,7 +1253,7 @@ Status build_parallel(const Sizes& sz, u64 seed, u64 c0, Network& net, cudaStrea
         s.post_count = P.post_count;
         s.post_off = P.post_off;
         s.third = P.third;
-        const u64 base_e = k == 1 ? tot_e[0] : 0, base_a = k == 1 ? tot_a[0] : 0, base_s = k == 1 ? tot_s[0] : 0;
+        const u64 base_e = 0, base_a = k == 1 ? tot_a[0] : 0, base_s = k == 1 ? tot_s[0] : 0;
         u32* e_src = k == 2 ? es.inh_src.get() : es.exc_src.get();
         u32* e_dst = k == 2 ? es.inh_dst.get() : es.exc_dst.get();
         emit_kernel<<<ceil_div(P.n_pres, 128), 128, 0, st>>>(s, orbits[k].get(), P.n_pres, P.self_mode, P.self_off,
@@ -882,6 +1276,11 @@ Status build_parallel(const Sizes& sz, u64 seed, u64 c0, Network& net, cudaStrea
     pc.mark("count + emit");
     const u64 counts[4] = {es.cap_exc, es.cap_inh, cap_e2a, cap_sic};
     AS_TRY(edge_lists_to_network(es.view(), counts, net, st));
+    net.fwd_exc_rs = std::move(fwd_exc_rs);
+    net.fwd_exc_dst = std::move(es.exc_dst);
+    net.fwd_inh_rs = std::move(fwd_inh_rs);
+    net.fwd_inh_dst = std::move(es.inh_dst);
+    net.has_fwd = true;
     pc.mark("CSR sort");
 
     // The astrocyte out-degree cap (src/astrosim_fused.cu:702) drops a third-factor

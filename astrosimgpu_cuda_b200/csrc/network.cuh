@@ -53,6 +53,19 @@ struct Network {
     // Edge counts of the whole network (exc, inh, e2a, sic), whatever `own` keeps.
     u64 total_edges[4] = {0, 0, 0, 0};
     bool partial() const { return !own.whole(sz); }
+    // Source-major lists of the exc and inh CSRs, when the builder wrote them while
+    // emitting the edges (the chunked builder): row r of fwd_exc (exc source r) and of
+    // fwd_inh (inh source r) lists the target rows of its edges in ascending order,
+    // the lists the windowed engine would otherwise derive by sorting the CSRs.
+    DevBuf<u32> fwd_exc_rs, fwd_exc_dst, fwd_inh_rs, fwd_inh_dst;
+    bool has_fwd = false;
+    void drop_forward() {
+        fwd_exc_rs.release();
+        fwd_exc_dst.release();
+        fwd_inh_rs.release();
+        fwd_inh_dst.release();
+        has_fwd = false;
+    }
     // Per-cell parameters (src/astrosim_fused.cu:917-933), always double.
     DevBuf<double> Ca_tot, IP3_0, tau_IP3, delta_IP3, V_reset, b;
     double build_seconds = 0.0;

@@ -241,6 +241,7 @@ Status Simulation::create(const astrosim_config& cfg, const char* biology_json, 
                 rc.n_neurons < (1u << 27) &&  // spike-list entries pack the neuron id in 27 bits
                 !(stepper && std::strcmp(stepper, "plain") == 0);
     if (!windowed_) {
+        net_.drop_forward();  // the per-step path reads only the target CSRs
         AS_TRY(st_.spike_bits.alloc_zero(static_cast<u64>(rc.slots) * rc.words, stream_));
         AS_TRY(st_.spike_val_raw.alloc_zero(static_cast<u64>(rc.slots) * nN * rbytes, stream_));
         AS_TRY(st_.sic_ring_raw.alloc_zero(static_cast<u64>(rc.slots) * nA * rbytes, stream_));

@@ -146,8 +146,29 @@ Status window_setup(const RunConsts& rc, Network& net, bool fp32, WindowState& w
     const size_t rb = fp32 ? sizeof(float) : sizeof(double);
     const size_t db = fp32 ? sizeof(Deposit<float>) : sizeof(Deposit<double>);
     // a rank of a sharded network keeps its own cells' rows: its forward lists reach its own cells only
-    AS_TRY(invert_csr(net.exc, net.own.n_lo, rc.n_exc, ws.fwd.exc_rs, ws.fwd.exc_dst, nullptr, st));
-    AS_TRY(invert_csr(net.inh, net.own.n_lo, net.sz.n_inh, ws.fwd.inh_rs, ws.fwd.inh_dst, nullptr, st));
+    if (net.has_fwd && net.fwd_exc_rs.size() == static_cast<size_t>(rc.n_exc) + 1 &&
+        net.fwd_inh_rs.size() == static_cast<size_t>(net.sz.n_inh) + 1) {
+        // the builder wrote these lists while emitting the edges, with the owned rows'
+        // indices (cell - n_lo); the forward lists hold target ids
+        ws.fwd.exc_rs = std::move(net.fwd_exc_rs);
+        ws.fwd.exc_dst = std::move(net.fwd_exc_dst);
+        ws.fwd.inh_rs = std::move(net.fwd_inh_rs);
+        ws.fwd.inh_dst = std::move(net.fwd_inh_dst);
+        net.has_fwd = false;
+        if (net.own.n_lo) {
+            if (net.exc.n_edges)
+                add_offset_kernel<<<ceil_div(net.exc.n_edges, 256), 256, 0, st>>>(ws.fwd.exc_dst.get(),
+                                                                                 net.exc.n_edges, net.own.n_lo);
+            if (net.inh.n_edges)
+                add_offset_kernel<<<ceil_div(net.inh.n_edges, 256), 256, 0, st>>>(ws.fwd.inh_dst.get(),
+                                                                                 net.inh.n_edges, net.own.n_lo);
+            AS_CUDA(cudaGetLastError());
+        }
+    } else {
+        net.drop_forward();
+        AS_TRY(invert_csr(net.exc, net.own.n_lo, rc.n_exc, ws.fwd.exc_rs, ws.fwd.exc_dst, nullptr, st));
+        AS_TRY(invert_csr(net.inh, net.own.n_lo, net.sz.n_inh, ws.fwd.inh_rs, ws.fwd.inh_dst, nullptr, st));
+    }
     AS_TRY(invert_csr(net.e2a, net.own.a_lo, rc.n_exc, ws.fwd.e2a_rs, ws.fwd.e2a_astro, &ws.fwd.e2a_pos, st));
     AS_TRY(invert_csr(net.sic, net.own.n_lo, rc.n_astro, ws.fwd.sic_rs, ws.fwd.sic_dst, nullptr, st));
     // Windows with more spikes than this use the pull gather instead of deposits.
