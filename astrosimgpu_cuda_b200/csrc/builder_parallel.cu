@@ -44,7 +44,6 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
-#include <cstdlib>
 #include <map>
 #include <vector>
 
@@ -630,41 +629,92 @@ __global__ void count_kernel(Sec s, const u64* orbit, u64 n, int self_mode, u32 
     }
 }
 
+// One output stream of one emitting thread: values go to p[o], p[o + 1], ...  Whole
+// 32-byte sectors leave as two 16-byte stores from an 8-value buffer in shared
+// memory; only the partial sectors at the two ends of a pre's run get single
+// stores.  With a single 4-byte store per value, L2 held partly written sectors
+// and filled each from DRAM before writing it back: at N = 3e6 the E block's
+// emission moved 32 GB of DRAM traffic for about 1.7 GB of edges.  The buffer is
+// stream-major in shared memory (value k of thread t at buf[k * kEmitBlock]), so
+// lanes at the same fill level hit different banks.
+constexpr u32 kEmitBlock = 128;
+
+struct SectorWriter {
+    u32* p;
+    u64 o;
+    u32* buf;
+    u32 k;
+    __device__ __forceinline__ void put(u32 v) {
+        if (k == 0 && (reinterpret_cast<unsigned long long>(p + o) & 31u)) {  // up to the next sector boundary
+            p[o++] = v;
+            return;
+        }
+        buf[k * kEmitBlock] = v;
+        if (++k == 8) {
+            const uint4 a = make_uint4(buf[0], buf[kEmitBlock], buf[2 * kEmitBlock], buf[3 * kEmitBlock]);
+            const uint4 b = make_uint4(buf[4 * kEmitBlock], buf[5 * kEmitBlock], buf[6 * kEmitBlock],
+                                       buf[7 * kEmitBlock]);
+            *reinterpret_cast<uint4*>(p + o) = a;
+            *reinterpret_cast<uint4*>(p + o + 4) = b;
+            o += 8;
+            k = 0;
+        }
+    }
+    __device__ __forceinline__ void flush() {
+        for (u32 i = 0; i < k; ++i) p[o + i] = buf[i * kEmitBlock];
+        o += k;
+        k = 0;
+    }
+};
+
+// The edges of one pre.  The sources of the exc, inh and e2a lists are the pre
+// itself and are filled in afterwards (fill_rows_kernel); the sic list's sources
+// are astrocytes and are written here.
 struct EmitVisit {
     Owned own;
-    u32 pre;
-    u32 *e_src, *e_dst, *t_src, *t_dst, *s_src, *s_dst;
-    u64 oe, oa, os;
+    SectorWriter e_dst, t_dst, s_src, s_dst;
     __device__ __forceinline__ void operator()(u32 post, bool hit, u32 astro) {
         const bool pn = own.neuron(post);
-        if (pn) {
-            e_src[oe] = pre;
-            e_dst[oe] = post - own.n_lo;
-            ++oe;
-        }
+        if (pn) e_dst.put(post - own.n_lo);
         if (hit) {
-            if (own.astro(astro)) {
-                t_src[oa] = pre;
-                t_dst[oa] = astro - own.a_lo;
-                ++oa;
-            }
+            if (own.astro(astro)) t_dst.put(astro - own.a_lo);
             if (pn) {
-                s_src[os] = astro;
-                s_dst[os] = post - own.n_lo;
-                ++os;
+                s_src.put(astro);
+                s_dst.put(post - own.n_lo);
             }
         }
     }
 };
 
-__global__ void emit_kernel(Sec s, const u64* orbit, u64 n, int self_mode, u32 self_off, Owned own, const u64* oe,
-                            const u64* oa, const u64* os, u64 base_e, u64 base_a, u64 base_s, u32* e_src,
-                            u32* e_dst, u32* t_src, u32* t_dst, u32* s_src, u32* s_dst) {
+__global__ void __launch_bounds__(kEmitBlock) emit_kernel(Sec s, const u64* orbit, u64 n, int self_mode,
+                                                          u32 self_off, Owned own, const u64* oe, const u64* oa,
+                                                          const u64* os, u64 base_e, u64 base_a, u64 base_s,
+                                                          u32* e_dst, u32* t_dst, u32* s_src, u32* s_dst) {
+    __shared__ u32 sbuf[4 * 8 * kEmitBlock];
     const u64 r = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (r >= n) return;
-    EmitVisit v{own, static_cast<u32>(r), e_src, e_dst, t_src, t_dst, s_src, s_dst,
-                base_e + oe[r], base_a + oa[r], base_s + os[r]};
+    u32* b = sbuf + threadIdx.x;
+    EmitVisit v{own,
+                SectorWriter{e_dst, base_e + oe[r], b, 0u},
+                SectorWriter{t_dst, base_a + oa[r], b + 8 * kEmitBlock, 0u},
+                SectorWriter{s_src, base_s + os[r], b + 16 * kEmitBlock, 0u},
+                SectorWriter{s_dst, base_s + os[r], b + 24 * kEmitBlock, 0u}};
     walk_pre(s, orbit[r], self_post_of(self_mode, static_cast<u32>(r), self_off), v);
+    v.e_dst.flush();
+    v.t_dst.flush();
+    v.s_src.flush();
+    v.s_dst.flush();
+}
+
+// out[i] = r for every i of row r, rows [base + o[r], base + o[r + 1]) (the last one
+// ends at base + total): the source lists whose source is the row's pre.  One warp
+// per row, so the writes are coalesced.
+__global__ void fill_rows_kernel(const u64* o, u64 n, u64 base, u64 total, u32* out) {
+    const u64 t = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const u64 r = t >> 5;
+    if (r >= n) return;
+    const u64 b = base + o[r], e = base + (r + 1 < n ? o[r + 1] : total);
+    for (u64 i = b + (threadIdx.x & 31u); i < e; i += 32) out[i] = static_cast<u32>(r);
 }
 
 __global__ void section_end_kernel(Sec s, const u64* orbit, u64 last, int self_mode, u32 self_off, u64* end) {
@@ -1254,14 +1304,23 @@ Status build_parallel(const Sizes& sz, u64 seed, u64 c0, Network& net, cudaStrea
         s.post_off = P.post_off;
         s.third = P.third;
         const u64 base_e = 0, base_a = k == 1 ? tot_a[0] : 0, base_s = k == 1 ? tot_s[0] : 0;
-        u32* e_src = k == 2 ? es.inh_src.get() : es.exc_src.get();
         u32* e_dst = k == 2 ? es.inh_dst.get() : es.exc_dst.get();
-        emit_kernel<<<ceil_div(P.n_pres, 128), 128, 0, st>>>(s, orbits[k].get(), P.n_pres, P.self_mode, P.self_off,
-                                                            own, oe[k].get(), oa[k].get(), os[k].get(), base_e,
-                                                            base_a, base_s, e_src, e_dst, es.e2a_src.get(),
-                                                            es.e2a_dst.get(), es.sic_src.get(), es.sic_dst.get());
+        emit_kernel<<<ceil_div(P.n_pres, kEmitBlock), kEmitBlock, 0, st>>>(
+            s, orbits[k].get(), P.n_pres, P.self_mode, P.self_off, own, oe[k].get(), oa[k].get(), os[k].get(),
+            base_e, base_a, base_s, e_dst, es.e2a_dst.get(), es.sic_src.get(), es.sic_dst.get());
         AS_CUDA(cudaGetLastError());
     }
+    // the pre-index sources: exc (both blocks, source-major), inh, and e2a (E block, then I block)
+    const auto fill = [&](const DevBuf<u64>& o, u64 n, u64 base, u64 total, u32* out) -> Status {
+        if (n == 0 || total == 0) return Status::Ok();
+        fill_rows_kernel<<<ceil_div(n * 32, 256), 256, 0, st>>>(o.get(), n, base, total, out);
+        AS_CUDA(cudaGetLastError());
+        return Status::Ok();
+    };
+    AS_TRY(fill(oe[0], plans[0].n_pres, 0, tot_e[0] + tot_e[1], es.exc_src.get()));
+    AS_TRY(fill(oe[2], plans[2].n_pres, 0, tot_e[2], es.inh_src.get()));
+    AS_TRY(fill(oa[0], plans[0].n_pres, 0, tot_a[0], es.e2a_src.get()));
+    AS_TRY(fill(oa[1], plans[1].n_pres, tot_a[0], tot_a[1], es.e2a_src.get()));
     int herr = 0;
     AS_TRY(read_err(err, &herr, st));
     if (herr) return make_error(ASTROSIM_ERR_CUDA, "edge emission failed (flags %d)", herr);
