@@ -380,6 +380,14 @@ void PhaseClock::mark(const char* what) {
     t0 = t;
 }
 
+double PhaseClock::now() { return now_s(); }
+
+void PhaseClock::mark_since(const char* what, double t) {
+    if (!on) return;
+    cudaStreamSynchronize(st);
+    std::fprintf(stderr, "[astrosim build] %-28s %8.3f ms\n", what, (now_s() - t) * 1e3);
+}
+
 Status build_network(const Sizes& sz, u64 seed, const Biology& bio, const BuildOptions& opt, Network& net,
                      cudaStream_t st) {
     PhaseClock pc(st);

@@ -74,6 +74,9 @@ struct PhaseClock {
     double t0;
     explicit PhaseClock(cudaStream_t s);
     void mark(const char* what);
+    // Prints the time since t (a PhaseClock::now() reading) under the same switch.
+    void mark_since(const char* what, double t);
+    static double now();
 };
 
 Status build_sequential(const Sizes& sz, u64 seed, u64 c0, Network& net, cudaStream_t st);

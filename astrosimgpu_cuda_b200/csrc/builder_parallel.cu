@@ -190,11 +190,10 @@ __global__ void table_kernel(Sec s, u64 sec_start, u32 chunk_len, u32 delta, u64
 // walks 5-10 chains.  Here a warp takes a chunk, its lanes take the candidates a few
 // at a time (a lane whose walk merged or left the chunk takes the next candidate),
 // claims go to a per-warp table in global memory, and once every candidate has
-// started and at most kSwarmHandoff walks remain, the warp hands them to a
+// started and at most `handoff` walks remain, the warp hands them to a
 // one-thread-per-walk kernel and takes the next chunk.  A walk's exit and count are
 // the same whoever it merges into, so the tables are identical.
 constexpr u32 kSwarmSlots = 4096;  // claim slots per warp (32 KB of global memory)
-constexpr u32 kSwarmHandoff = 4;
 constexpr u32 kSwarmIdle = 0xFFFFFFFFu;
 
 struct SwarmRec {
@@ -211,8 +210,9 @@ struct SwarmCont {
 };
 
 __global__ void __launch_bounds__(128) swarm_kernel(Sec s, u64 sec_start, u32 chunk_len, u32 delta, u32 n_chunks,
-                                                    unsigned* next_chunk, unsigned long long* tables, SwarmRec rec,
-                                                    SwarmCont* cont, unsigned* n_cont, unsigned cont_cap) {
+                                                    u32 handoff, unsigned* next_chunk, unsigned long long* tables,
+                                                    SwarmRec rec, SwarmCont* cont, unsigned* n_cont,
+                                                    unsigned cont_cap) {
     const u32 lane = threadIdx.x & 31u;
     const u64 warp = (static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     unsigned long long* tab = tables + warp * kSwarmSlots;
@@ -283,7 +283,7 @@ __global__ void __launch_bounds__(128) swarm_kernel(Sec s, u64 sec_start, u32 ch
             }
             const unsigned live = __ballot_sync(0xffffffffu, w != kSwarmIdle);
             if (live == 0) break;
-            if (next >= delta && static_cast<u32>(__popc(live)) <= kSwarmHandoff) {
+            if (next >= delta && static_cast<u32>(__popc(live)) <= handoff) {
                 if (w != kSwarmIdle) {
                     const unsigned k = atomicAdd(n_cont, 1u);
                     if (k < cont_cap) cont[k] = SwarmCont{chunk, w, c, cnt, 0u};
@@ -837,22 +837,20 @@ u32 swarm_blocks_per_sm() {
 
 // The (exit, pres) table of every chunk candidate: t_exit/t_cnt[chunk * delta + d]
 // for the walk from tape position sec_start + chunk * chunk_len + d.
-// Long chunks (kSwarmMinChunk positions and up, the sections of networks from about
-// N = 2e5) go to the warp swarms; short ones to one CTA per chunk, which walks all
-// candidates at once and measured faster there (N = 2e3-3e4: 0.3 vs 1.3 ms per
-// section; N = 1e7: 268 ms vs 33 ms for the E block the other way round).
-constexpr u32 kSwarmMinChunk = 16384;
-
-Status chunk_tables(Sec s, u64 sec_start, u32 chunk_len, u32 delta, u32 n_chunks, u64* t_exit, u32* t_cnt,
-                    cudaStream_t st) {
-    if (chunk_len < kSwarmMinChunk) {
+// A section's chunks of swarm_min_chunk positions and more go to the warp swarms;
+// shorter ones (the shortened chunks of small networks) to one CTA per chunk, which
+// walks all candidates at once and measured faster there (N = 2e3-3e4: 0.3 vs 1.3
+// ms per section; N = 1e7: 268 ms vs 33 ms for the E block the other way round).
+Status chunk_tables(Sec s, u64 sec_start, u32 chunk_len, u32 delta, u32 n_chunks, u32 swarm_min_chunk, u32 handoff,
+                    u64* t_exit, u32* t_cnt, cudaStream_t st) {
+    if (chunk_len < swarm_min_chunk) {
         table_kernel<<<n_chunks, delta, 0, st>>>(s, sec_start, chunk_len, delta, t_exit, t_cnt);
         AS_CUDA(cudaGetLastError());
         return Status::Ok();
     }
     const u64 n = static_cast<u64>(n_chunks) * delta;
     const u32 blocks = std::max<u32>(1, std::min<u32>(ceil_div(n_chunks, 4), sm_count() * swarm_blocks_per_sm()));
-    const unsigned cont_cap = n_chunks * kSwarmHandoff;
+    const unsigned cont_cap = n_chunks * handoff;
     DevBuf<unsigned long long> tables;
     DevBuf<int> par;
     DevBuf<u32> mycnt, pcnt;
@@ -867,8 +865,8 @@ Status chunk_tables(Sec s, u64 sec_start, u32 chunk_len, u32 delta, u32 n_chunks
     AS_TRY(cont.alloc(cont_cap));
     AS_TRY(counters.alloc_zero(2, st));
     const SwarmRec rec{par.get(), mycnt.get(), pcnt.get(), ex.get()};
-    swarm_kernel<<<blocks, 128, 0, st>>>(s, sec_start, chunk_len, delta, n_chunks, counters.get(), tables.get(), rec,
-                                         cont.get(), counters.get() + 1, cont_cap);
+    swarm_kernel<<<blocks, 128, 0, st>>>(s, sec_start, chunk_len, delta, n_chunks, handoff, counters.get(),
+                                         tables.get(), rec, cont.get(), counters.get() + 1, cont_cap);
     AS_CUDA(cudaGetLastError());
     swarm_continue_kernel<<<ceil_div(cont_cap, 128), 128, 0, st>>>(s, sec_start, chunk_len, delta, cont.get(),
                                                                   counters.get() + 1, cont_cap, rec);
@@ -888,6 +886,16 @@ struct SectionPlan {
     int self_mode;  // 0: no autapse possible; 1: autapse at post == r + self_off
     u32 self_off;
     bool autapse_shifts_stream;
+    // Chunk tables by warp swarms from this chunk length up, handing off at most
+    // `handoff` walks per chunk.  The continuation and orbit walks are one serial
+    // walk per chunk, so their time follows the chunk length; the swarms' follows
+    // the number of chunks.  Measured per section (N = 3e6, ncu): shortening the I
+    // block's chunks (about 40 draws per pre) from 16384 to 4096 positions took its
+    // tables and orbit from 10.8 to 3.8 ms, and the inhibitory section's (about 80
+    // draws per pre, no third-factor draws) from 16384 to 8192 with hand-off at 6
+    // from 17.5 to 9.6 ms; the E block (about 150 draws per pre) keeps 32768 and 4
+    // (hand-off at 3: 16.9 instead of 14.4 ms).
+    u32 swarm_min_chunk, handoff;
 };
 
 // Finds the start of every pre of one section (steps 3 and 4 of the file comment).
@@ -926,7 +934,8 @@ Status section_orbit(const SectionPlan& P, Sec s, u64 start, DevBuf<int>& err, D
         AS_TRY(c_entry.alloc(n_chunks));
         AS_TRY(c_g0.alloc(n_chunks));
         AS_TRY(endg.alloc(1));
-        AS_TRY(chunk_tables(s, start, chunk_len, delta, n_chunks, t_exit.get(), t_cnt.get(), st));
+        AS_TRY(chunk_tables(s, start, chunk_len, delta, n_chunks, P.swarm_min_chunk, P.handoff, t_exit.get(),
+                            t_cnt.get(), st));
         group_compose_kernel<<<n_groups, delta, 0, st>>>(s, start, chunk_len, delta, n_chunks, t_exit.get(),
                                                          t_cnt.get(), g_exit.get(), g_cnt.get());
         AS_CUDA(cudaGetLastError());
@@ -1162,9 +1171,9 @@ Status build_parallel(const Sizes& sz, u64 seed, u64 c0, Network& net, cudaStrea
     // ---- 2. skip cache over every tape position the three sections can reach
     const double ne = sz.n_exc, ni = sz.n_inh, nn = nN, p = sz.p;
     SectionPlan plans[3] = {
-        {"E block", sz.n_exc, 0, 1, sz.n_exc, 1.0 + p * ne * (2.0 + kPThird), 32768, 384, 1, 0, true},
-        {"I block", sz.n_inh, sz.n_exc, 1, sz.n_exc, 1.0 + p * ni * (2.0 + kPThird), 16384, 192, 0, 0, false},
-        {"inhibitory", nN, 0, 0, sz.n_inh, 1.0 + p * nn, 16384, 192, 1, sz.n_exc, false},
+        {"E block", sz.n_exc, 0, 1, sz.n_exc, 1.0 + p * ne * (2.0 + kPThird), 32768, 384, 1, 0, true, 16384, 4},
+        {"I block", sz.n_inh, sz.n_exc, 1, sz.n_exc, 1.0 + p * ni * (2.0 + kPThird), 4096, 192, 0, 0, false, 4096, 4},
+        {"inhibitory", nN, 0, 0, sz.n_inh, 1.0 + p * nn, 8192, 192, 1, sz.n_exc, false, 8192, 6},
     };
     double est_total = 0.0;
     for (const auto& P : plans) est_total += static_cast<double>(P.n_pres) * P.draws_per_pre;

@@ -264,6 +264,7 @@ Status Ensemble::create(const astrosim_config* cfgs, u32 n, const char* const* b
     for (u32 t = 1; t < workers; ++t) pool.emplace_back(work);
     work();
     for (auto& th : pool) th.join();
+    const auto t_built = std::chrono::steady_clock::now();
     for (u32 i = 0; i < n; ++i)
         if (!st[i].ok()) return make_error(st[i].code, "network %u: %s", i, st[i].msg.c_str());
     for (u32 i = 0; i < n; ++i)
@@ -278,7 +279,12 @@ Status Ensemble::create(const astrosim_config* cfgs, u32 n, const char* const* b
     AS_TRY(stop_.alloc(n));
     AS_CUDA(cudaMemcpyAsync(stop_.get(), stops.data(), n * sizeof(i64), cudaMemcpyHostToDevice, stream_));
     AS_TRY(rebuild());
-    build_seconds_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    const auto t_end = std::chrono::steady_clock::now();
+    build_seconds_ = std::chrono::duration<double>(t_end - t0).count();
+    if (std::getenv("ASTROSIM_TIMING"))
+        std::fprintf(stderr, "[astrosim ensemble] %u networks on %u threads %.3f ms, descriptors and tiles %.3f ms\n", n,
+                     workers, std::chrono::duration<double, std::milli>(t_built - t0).count(),
+                     std::chrono::duration<double, std::milli>(t_end - t_built).count());
     return Status::Ok();
 }
 

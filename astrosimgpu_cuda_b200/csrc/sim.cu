@@ -148,6 +148,7 @@ Status Simulation::create(const astrosim_config& cfg, const char* biology_json, 
     if (cfg.device < 0 || cfg.device >= ndev)
         return make_error(ASTROSIM_ERR_INVALID_ARG, "device %d out of range (%d visible)", cfg.device, ndev);
     device_ = cfg.device;
+    const double t_create = PhaseClock::now();
     AS_CUDA(cudaSetDevice(device_));
     AS_CUDA(take_stream(device_, &stream_));
     keep_pool_memory(device_, 8ull << 30);
@@ -267,6 +268,7 @@ Status Simulation::create(const astrosim_config& cfg, const char* biology_json, 
     }
     AS_CUDA(cudaGetLastError());
     AS_CUDA(cudaStreamSynchronize(stream_));
+    PhaseClock(stream_).mark_since("simulation set-up (total)", t_create);
     return Status::Ok();
 }
 
