@@ -158,9 +158,21 @@ static int bits_for(u32 n) {
     return b;
 }
 
+// Scratch of the four sorts of one network: two key buffers and CUB's temporary
+// storage, allocated once for the largest list (the per-sort alternate buffers of
+// the plain SortPairs came to about 20 GB of allocations at N = 1e7).
+struct SortScratch {
+    DevBuf<u32> ka, kb;
+    DevBuf<unsigned char> temp;
+};
+
 // Stable counting sort by target (src/astrosim_fused.cu:307-314).  The input lists
 // are in emission order; an LSD radix sort is stable, so each row keeps that order.
-Status edges_to_csr(const u32* src, const u32* dst, u64 n, u32 n_targets, DeviceCSR& out, cudaStream_t st) {
+// The source list is consumed (it is one of the sort's two value buffers).  With
+// keep_dst the target list is copied into the scratch first and survives (the exc
+// and inh lists are kept as forward lists); otherwise it is sorted in place.
+Status edges_to_csr(u32* src, u32* dst, u64 n, u32 n_targets, bool keep_dst, SortScratch& sc, DeviceCSR& out,
+                    cudaStream_t st) {
     out.n_targets = n_targets;
     out.n_edges = n;
     AS_TRY(out.row_start.alloc(static_cast<size_t>(n_targets) + 1));
@@ -169,17 +181,20 @@ Status edges_to_csr(const u32* src, const u32* dst, u64 n, u32 n_targets, Device
         AS_CUDA(cudaMemsetAsync(out.row_start.get(), 0, (static_cast<size_t>(n_targets) + 1) * sizeof(u32), st));
         return Status::Ok();
     }
-    DevBuf<u32> keys_out;
-    AS_TRY(keys_out.alloc(n));
-    size_t temp_bytes = 0;
+    u32* k_cur = dst;
+    u32* k_alt = sc.ka.get();
+    if (keep_dst) {
+        AS_CUDA(cudaMemcpyAsync(sc.ka.get(), dst, n * sizeof(u32), cudaMemcpyDeviceToDevice, st));
+        k_cur = sc.ka.get();
+        k_alt = sc.kb.get();
+    }
+    cub::DoubleBuffer<u32> keys(k_cur, k_alt), vals(src, out.src.get());
     const int end_bit = bits_for(n_targets);
-    AS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, dst, keys_out.get(), src, out.src.get(), n, 0,
-                                            end_bit, st));
-    DevBuf<unsigned char> temp;
-    AS_TRY(temp.alloc(temp_bytes));
-    AS_CUDA(cub::DeviceRadixSort::SortPairs(temp.get(), temp_bytes, dst, keys_out.get(), src, out.src.get(), n, 0,
-                                            end_bit, st));
-    row_start_kernel<<<ceil_div(static_cast<u64>(n_targets) + 1, 256), 256, 0, st>>>(keys_out.get(), n, n_targets,
+    size_t temp_bytes = sc.temp.bytes();
+    AS_CUDA(cub::DeviceRadixSort::SortPairs(sc.temp.get(), temp_bytes, keys, vals, n, 0, end_bit, st));
+    if (vals.Current() != out.src.get())
+        AS_CUDA(cudaMemcpyAsync(out.src.get(), vals.Current(), n * sizeof(u32), cudaMemcpyDeviceToDevice, st));
+    row_start_kernel<<<ceil_div(static_cast<u64>(n_targets) + 1, 256), 256, 0, st>>>(keys.Current(), n, n_targets,
                                                                                    out.row_start.get());
     AS_CUDA(cudaGetLastError());
     AS_CUDA(cudaStreamSynchronize(st));
@@ -188,10 +203,24 @@ Status edges_to_csr(const u32* src, const u32* dst, u64 n, u32 n_targets, Device
 
 Status edge_lists_to_network(const EdgeLists& e, const u64 counts[4], Network& net, cudaStream_t st) {
     const u32 nn = net.own.n_hi - net.own.n_lo, na = net.own.a_hi - net.own.a_lo;
-    AS_TRY(edges_to_csr(e.exc_src, e.exc_dst, counts[0], nn, net.exc, st));
-    AS_TRY(edges_to_csr(e.inh_src, e.inh_dst, counts[1], nn, net.inh, st));
-    AS_TRY(edges_to_csr(e.e2a_src, e.e2a_dst, counts[2], na, net.e2a, st));
-    AS_TRY(edges_to_csr(e.sic_src, e.sic_dst, counts[3], nn, net.sic, st));
+    const u32 n_targets[4] = {nn, nn, na, nn};
+    const u64 n_max = std::max(std::max(counts[0], counts[1]), std::max(counts[2], counts[3]));
+    SortScratch sc;
+    AS_TRY(sc.ka.alloc(n_max));
+    AS_TRY(sc.kb.alloc(std::max(counts[0], counts[1])));
+    size_t temp_bytes = 1;
+    for (int k = 0; k < 4; ++k) {
+        if (counts[k] == 0) continue;
+        size_t b = 0;
+        cub::DoubleBuffer<u32> keys(sc.ka.get(), sc.kb.get()), vals(sc.ka.get(), sc.kb.get());
+        AS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b, keys, vals, counts[k], 0, bits_for(n_targets[k]), st));
+        temp_bytes = std::max(temp_bytes, b);
+    }
+    AS_TRY(sc.temp.alloc(temp_bytes));
+    AS_TRY(edges_to_csr(e.exc_src, e.exc_dst, counts[0], nn, true, sc, net.exc, st));
+    AS_TRY(edges_to_csr(e.inh_src, e.inh_dst, counts[1], nn, true, sc, net.inh, st));
+    AS_TRY(edges_to_csr(e.e2a_src, e.e2a_dst, counts[2], na, false, sc, net.e2a, st));
+    AS_TRY(edges_to_csr(e.sic_src, e.sic_dst, counts[3], nn, false, sc, net.sic, st));
     return Status::Ok();
 }
 

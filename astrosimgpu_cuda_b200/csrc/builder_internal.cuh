@@ -27,9 +27,9 @@ struct EdgeStorage {
 Status alloc_edge_lists(const Sizes& sz, EdgeStorage& s, cudaStream_t st);
 // Sorts the lists into the four CSRs.  counts: exc, inh, e2a, sic list lengths; the
 // destinations are row indices of net.own (cell - lo), and the CSRs get the rows of
-// the owned cells.
+// the owned cells.  The source lists and the e2a and sic target lists are used as
+// sort buffers (their contents are lost); the exc and inh target lists survive.
 Status edge_lists_to_network(const EdgeLists& e, const u64 counts[4], Network& net, cudaStream_t st);
-Status edges_to_csr(const u32* src, const u32* dst, u64 n, u32 n_targets, DeviceCSR& out, cudaStream_t st);
 // Keeps rows [lo, hi) of a CSR (row r of the result is row lo + r of the input).
 Status slice_csr(DeviceCSR& c, u32 lo, u32 hi, cudaStream_t st);
 
