@@ -1053,7 +1053,10 @@ Status section_orbit(const SectionPlan& P, Sec s, u64 start, DevBuf<int>& err, D
             const u64 t_autapse = static_cast<u64>(static_cast<long long>(h.r) + d);
             pieces.push_back(Piece{expl.get() + static_cast<u64>(i) * max_explicit, t_autapse, m.m});
             u64 walked = m.m;
-            for (u32 cap = 4096; m.capped;) {  // this walk is on the chain: continue it
+            // This walk is on the chain: continue it from where it stopped (its tape
+            // position and true index are all the state it has), in pieces of growing
+            // size, until it rejoins the table orbit or the section ends.
+            for (u32 cap = 4096; m.capped; cap = std::min<u32>(cap * 8, 1u << 24)) {
                 DevBuf<u64> buf;
                 AS_TRY(buf.alloc(cap));
                 remerge_continue_kernel<<<1, 1, 0, st>>>(s, m.c_next, m.r_next, forbit.get(), target, P.n_pres, cap,
@@ -1061,15 +1064,10 @@ Status section_orbit(const SectionPlan& P, Sec s, u64 start, DevBuf<int>& err, D
                 AS_CUDA(cudaGetLastError());
                 Remerge m2{};
                 AS_TRY(to_host(&m2, cont_res.get(), 1, st));
-                if (m2.capped && cap < (1u << 24)) {
-                    cap *= 8;  // the same continuation again with more room
-                    continue;
-                }
                 pieces.push_back(Piece{buf.get(), t_autapse + walked, m2.m});
                 walked += m2.m;
                 cont_starts.push_back(std::move(buf));
                 m = m2;
-                break;
             }
             if (!m.ok) return make_error(ASTROSIM_ERR_CUDA, "%s: re-merge walk incomplete", P.name);
             if (m.k < 0) {
