@@ -54,6 +54,8 @@ private:
     void launch_window(int v);  // window + push kernels for variant v
 
     std::vector<std::unique_ptr<Simulation>> nets_;
+    std::vector<cudaStream_t> build_streams_;  // lent to the networks create() built
+    int build_device_ = 0;
     std::vector<i64> win_host_;  // window index of each network at the last sync
     bool fp32_ = false;
     int W_ = 0;

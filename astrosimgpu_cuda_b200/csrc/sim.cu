@@ -120,7 +120,7 @@ Simulation::~Simulation() {
     net_ = Network();
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
-    if (stream_) {
+    if (stream_ && stream_owned_) {
         if (cudaStreamSynchronize(stream_) == cudaSuccess) give_stream(device_, stream_);
         else cudaStreamDestroy(stream_);
     }
@@ -150,9 +150,10 @@ Status Simulation::create(const astrosim_config& cfg, const char* biology_json, 
     device_ = cfg.device;
     const double t_create = PhaseClock::now();
     AS_CUDA(cudaSetDevice(device_));
-    AS_CUDA(take_stream(device_, &stream_));
+    if (!stream_) AS_CUDA(take_stream(device_, &stream_));
     keep_pool_memory(device_, 8ull << 30);
     AllocStream alloc_scope(stream_);
+    PhaseClock(stream_).mark_since("stream", t_create);
 
     {
         Biology base;  // the reference's constants, then the JSON overrides, then cfg's fields

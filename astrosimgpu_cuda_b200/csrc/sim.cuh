@@ -116,6 +116,13 @@ public:
     // own: the cells whose connectivity rows this network keeps (a rank of a sharded
     // network); null keeps the whole network.  Only the owned cells may be stepped.
     Status create(const astrosim_config& cfg, const char* biology_json = nullptr, const CellRange* own = nullptr);
+    // Before create: run on stream s, which the caller owns and keeps alive for as
+    // long as this simulation exists (other simulations may share it), instead of a
+    // stream of this simulation's own.
+    void lend_stream(cudaStream_t s) {
+        stream_ = s;
+        stream_owned_ = false;
+    }
     Status step(i64 n);
     Status summary(astrosim_summary_t& out);
     Status spike_counts(i64 first, i64 n, u32* dst);
@@ -165,6 +172,7 @@ private:
     RunConsts rc_{};
     StateBuffers st_;
     cudaStream_t stream_ = nullptr;
+    bool stream_owned_ = true;
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     bool have_step_events_ = false;
     int device_ = 0;

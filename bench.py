@@ -617,6 +617,12 @@ def main():
 
     if args.leg:  # one form alone, for profiling captures
         if ws == 1:
+            # The process set-up the full run does first (CUDA context, first use of the
+            # kernels), so that the leg times its own work as it does inside the full run;
+            # otherwise it counts about 1.2 s of context creation as network builds.
+            import astrosimgpu_cuda_b200 as asg
+            with asg.Simulation(n_total=30000, seed=SEED, pre_ms=0, sim_ms=2, precision="fp32") as warm:
+                warm.step(20)
             leg = run_ensemble(args) if args.leg == "ensemble" else serving_sweep(args)
             print(json.dumps({"leg": args.leg, args.leg: leg}), flush=True)
         return
