@@ -44,6 +44,8 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdlib>
+#include <cstring>
 #include <map>
 #include <vector>
 
@@ -843,7 +845,14 @@ u32 swarm_blocks_per_sm() {
 // ms per section; N = 1e7: 268 ms vs 33 ms for the E block the other way round).
 Status chunk_tables(Sec s, u64 sec_start, u32 chunk_len, u32 delta, u32 n_chunks, u32 swarm_min_chunk, u32 handoff,
                     u64* t_exit, u32* t_cnt, cudaStream_t st) {
-    if (chunk_len < swarm_min_chunk) {
+    // ASTROSIM_CHUNK_TABLES=cta|swarm forces one of the two (exact, equivalent) table
+    // algorithms; the tests build the same networks both ways.
+    bool cta = chunk_len < swarm_min_chunk;
+    if (const char* env = std::getenv("ASTROSIM_CHUNK_TABLES")) {
+        if (std::strcmp(env, "cta") == 0) cta = true;
+        else if (std::strcmp(env, "swarm") == 0) cta = false;
+    }
+    if (cta) {
         table_kernel<<<n_chunks, delta, 0, st>>>(s, sec_start, chunk_len, delta, t_exit, t_cnt);
         AS_CUDA(cudaGetLastError());
         return Status::Ok();

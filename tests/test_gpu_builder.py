@@ -66,3 +66,22 @@ def test_sequential_and_parallel_paths_agree_on_parameters(builder):
             np.testing.assert_array_equal(a[1], b[1])
         else:
             np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("n_total,seed", [(300000, 1), (300000, 2), (300000, 3), (2000, 5)])
+def test_swarm_and_cta_chunk_tables_give_the_same_network(n_total, seed, builder, monkeypatch):
+    """The chunk tables come from persistent warp swarms (long chunks) or one CTA per
+    chunk (short ones); both are exact.  N = 3e5 runs the swarms on its E- and
+    I-block chunks by default and the CTA kernel on its inhibitory ones, N = 2e3 the
+    CTA kernel throughout; each network is built both ways here and must come out
+    identical."""
+    builder("parallel")
+    out = {}
+    for how in ("swarm", "cta"):
+        monkeypatch.setenv("ASTROSIM_CHUNK_TABLES", how)
+        with asg.Simulation(n_total=n_total, seed=seed, pre_ms=0, sim_ms=0) as sim:
+            out[how] = [sim.csr(k) for k in ("exc", "inh", "sic", "e2a")]
+    for k, (a, b) in enumerate(zip(out["swarm"], out["cta"])):
+        assert a[1].size > 0, k
+        np.testing.assert_array_equal(a[0], b[0])
+        np.testing.assert_array_equal(a[1], b[1])
