@@ -12,6 +12,7 @@
 #include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
+#include <thread>
 #include <chrono>
 #include <cmath>
 #include <cstdlib>
@@ -417,6 +418,49 @@ void PhaseClock::mark_since(const char* what, double t) {
     std::fprintf(stderr, "[astrosim build] %-28s %8.3f ms\n", what, (now_s() - t) * 1e3);
 }
 
+namespace {
+
+// A host thread running one stream-ordered job on a pooled stream of its own; every
+// path out joins it and returns the stream.
+class ParamThread {
+public:
+    template <class F>
+    Status start(F job) {
+        AS_CUDA(cudaGetDevice(&dev_));
+        AS_CUDA(take_stream(dev_, &st_));
+        th_ = std::thread([this, job] {
+            cudaSetDevice(dev_);
+            AllocStream scope(st_);
+            result_ = job(st_);
+            if (result_.ok()) {
+                const cudaError_t e = cudaStreamSynchronize(st_);
+                if (e != cudaSuccess) result_ = make_error(ASTROSIM_ERR_CUDA, "parameter draws: %s", cudaGetErrorString(e));
+            }
+        });
+        return Status::Ok();
+    }
+    Status finish() {
+        stop();
+        return result_;
+    }
+    ~ParamThread() { stop(); }
+
+private:
+    void stop() {
+        if (th_.joinable()) th_.join();
+        if (st_) {
+            give_stream(dev_, st_);
+            st_ = nullptr;
+        }
+    }
+    int dev_ = 0;
+    cudaStream_t st_ = nullptr;
+    std::thread th_;
+    Status result_;
+};
+
+}  // namespace
+
 Status build_network(const Sizes& sz, u64 seed, const Biology& bio, const BuildOptions& opt, Network& net,
                      cudaStream_t st) {
     PhaseClock pc(st);
@@ -437,6 +481,14 @@ Status build_network(const Sizes& sz, u64 seed, const Biology& bio, const BuildO
         else if (std::strcmp(env, "parallel") == 0) threshold = 0;
     }
     net.own = opt.own.clamped(sz);
+    // The cell parameters come from counter 0 of their own sequence of draws, so they
+    // do not depend on the connectivity walk: a second host thread draws them on a
+    // second stream while the walk runs (the walk's phases wait on the host between
+    // small kernels, which leaves the GPU room).  Their buffers are allocated here, on
+    // this thread's allocation stream, like the rest of the network.
+    AS_TRY(alloc_cell_parameters(sz, net));
+    ParamThread params;
+    AS_TRY(params.start([&](cudaStream_t ps) { return draw_cell_parameters(sz, seed, bio, net, ps); }));
     if (est <= static_cast<double>(threshold)) {
         // a small network: the one-thread walk builds every row, then the owned rows are kept
         net.builder_path = 0;
@@ -458,8 +510,8 @@ Status build_network(const Sizes& sz, u64 seed, const Biology& bio, const BuildO
         AS_TRY(build_parallel(sz, seed, c0, net, st));
     }
     pc.mark("connectivity");
-    AS_TRY(draw_cell_parameters(sz, seed, bio, net, st));
-    pc.mark("parameters");
+    AS_TRY(params.finish());
+    pc.mark("parameters (wait after the walk)");
     AS_CUDA(cudaStreamSynchronize(st));
     net.build_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     return Status::Ok();

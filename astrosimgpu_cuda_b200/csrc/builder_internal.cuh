@@ -81,6 +81,10 @@ struct PhaseClock {
 
 Status build_sequential(const Sizes& sz, u64 seed, u64 c0, Network& net, cudaStream_t st);
 Status build_parallel(const Sizes& sz, u64 seed, u64 c0, Network& net, cudaStream_t st);
+// The per-cell parameter buffers of net (on this thread's allocation stream), then
+// their draws on stream st (src/astrosim_fused.cu:917-933).  The draws touch no other
+// member of net.
+Status alloc_cell_parameters(const Sizes& sz, Network& net);
 Status draw_cell_parameters(const Sizes& sz, u64 seed, const Biology& bio, Network& net, cudaStream_t st);
 
 }  // namespace astrosim

@@ -345,7 +345,7 @@ __global__ void zero_scan_kernel(u64 seed, u64 n, unsigned* found) {
 
 }  // namespace
 
-Status draw_cell_parameters(const Sizes& sz, u64 seed, const Biology& bio, Network& net, cudaStream_t st) {
+Status alloc_cell_parameters(const Sizes& sz, Network& net) {
     const u32 nA = sz.n_astro, nN = sz.n_neurons;
     AS_TRY(net.Ca_tot.alloc(nA));
     AS_TRY(net.IP3_0.alloc(nA));
@@ -353,6 +353,11 @@ Status draw_cell_parameters(const Sizes& sz, u64 seed, const Biology& bio, Netwo
     AS_TRY(net.delta_IP3.alloc(nA));
     AS_TRY(net.V_reset.alloc(nN));
     AS_TRY(net.b.alloc(nN));
+    return Status::Ok();
+}
+
+Status draw_cell_parameters(const Sizes& sz, u64 seed, const Biology& bio, Network& net, cudaStream_t st) {
+    const u32 nA = sz.n_astro, nN = sz.n_neurons;
 
     // src/astrosim_fused.cu:919-924: four astrocyte parameters per cell, in this order
     Phase pa{};
