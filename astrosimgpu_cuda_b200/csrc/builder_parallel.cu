@@ -50,6 +50,7 @@
 #include <vector>
 
 #include "builder_internal.cuh"
+#include "pool_offsets.h"
 #include "walk.cuh"
 #include "walk_chunked.cuh"
 
@@ -795,18 +796,11 @@ Status guess_pool_prefix(u64 seed, u32 nN, u32 nA, u32 take, u64 c0, u64* prefix
     if (m > cap) return Status::Ok();  // leave the zero guess to the loop
     std::vector<PoolRedraw> h(m);
     if (m) AS_TRY(to_host(h.data(), list.get(), m, st));
-    std::sort(h.begin(), h.end(), [](const PoolRedraw& a, const PoolRedraw& b) { return a.t < b.t; });
+    std::vector<PoolRedrawAt> sorted(m);
+    for (unsigned i = 0; i < m; ++i) sorted[i] = PoolRedrawAt{h[i].t, h[i].extra};
+    std::sort(sorted.begin(), sorted.end(), [](const PoolRedrawAt& a, const PoolRedrawAt& b) { return a.t < b.t; });
     std::vector<u32> bq, be;
-    u64 next_start = c0, q_next = 0;
-    for (const PoolRedraw& b : h) {
-        if (b.t < next_start || (b.t - next_start) % take) continue;  // not a pool start
-        const u64 q = q_next + (b.t - next_start) / take;
-        if (q >= nN) break;
-        bq.push_back(static_cast<u32>(q));
-        be.push_back(b.extra);
-        q_next = q + 1;
-        next_start = b.t + take + b.extra;
-    }
+    pools_with_redraws(sorted, c0, take, nN, bq, be);
     if (bq.empty()) return Status::Ok();
     DevBuf<u64> extra;
     DevBuf<u32> dq, de;
